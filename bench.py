@@ -1,0 +1,497 @@
+"""Benchmark of the depth-map path: one step = one full-resolution view (4000 x 3000 reference,
+8 sources, 256 fronto-parallel inverse-depth planes over [60, 90] m, 7 x 7 ZNCC, best-2
+aggregation, winner-take-all + parabola) followed by 4 red-black PatchMatch iterations (7 x 7
+slanted window, step 1, normals seeded within 30 deg of vertical) on every pixel.
+
+Metric: ZNCC evaluations per second (pixel x hypothesis x source), reported in Gpix.plane.view/s.
+The sweep contributes H W planes sources; each PatchMatch iteration contributes H W x 11
+hypotheses (current + 8 propagated + 2 random, nominal) x sources.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision fp32|fp16]
+
+N > 1 (torchrun): every rank sweeps its own seeded view (weak scaling, no collective on the data
+path); time = max over ranks (all_reduce MAX of device-event times).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PM_HYPS = 11          # hypotheses per PatchMatch pixel-iteration (1 + 8 propagation + 2 random)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--config", default="c2")
+    ap.add_argument("--width", type=int, default=0, help="override the image width (smaller test runs)")
+    ap.add_argument("--height", type=int, default=0)
+    ap.add_argument("--planes", type=int, default=0)
+    ap.add_argument("--pm-iters", type=int, default=-1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(a):
+    from py_ortho_b200 import scene as S
+    cfg = S.CONFIGS[a.config]
+    W = a.width or cfg.width
+    H = a.height or cfg.height
+    planes = a.planes or cfg.planes
+    iters = cfg.pm_iters if a.pm_iters < 0 else a.pm_iters
+    return cfg, W, H, planes, iters
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples (200 ms) during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu, self.proc, self.lines = gpu, None, []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.t.join(timeout=2)
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ our arm
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+    from py_ortho_b200 import _lib as L
+    from py_ortho_b200 import dense, fast, scene as S
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    L.load()
+    cfg, W, H, nplanes, iters = workload(a)
+    prec = L.PREC_FP16 if a.precision == "fp16" else L.PREC_FP32
+    t0 = time.time()
+    sc = S.make_scene(cfg, seed=rank, device=dev, width=W, height=H)
+    planes = S.plane_list(cfg.depth_range[0], cfg.depth_range[1], nplanes)
+    ref_h = sc.grey(sc.ref)
+    srcs_h = [sc.grey(s) for s in sc.srcs]
+    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+    r, top_k = cfg.radius, cfg.top_k
+    nsrc = len(srcs_h)
+    ref = torch.from_numpy(ref_h).to(dev)
+    srcs = [torch.from_numpy(s).to(dev) for s in srcs_h]
+    srcs_k = [fast.to_fp16(s) for s in srcs] if prec == L.PREC_FP16 else srcs
+    mu = torch.empty_like(ref)
+    sd = torch.empty_like(ref)
+    L.check(L.load().mvs_ref_stats(H, W, ref.data_ptr(), r, mu.data_ptr(), sd.data_ptr(), L.stream_handle()))
+    ray = fast.rays_world((H, W), sc.ref_cam)
+    normal0 = torch.from_numpy(S.tilted_normals(H, W, 1000 + rank)).to(dev)
+    active = torch.ones((H, W), dtype=torch.uint8, device=dev)
+    hyp = dense.Hypotheses.planes_inv(planes)
+    ref_cam = sc.ref_cam.row()
+    par = np.array([c.row() for c in sc.src_cams], np.float64)
+    Cr = np.asarray(sc.ref_cam.C, np.float64)
+    near, far = cfg.depth_range
+    state = dense.new_state(H, W, dev)
+    depth = torch.empty((H, W), dtype=torch.float32, device=dev)
+    normal = torch.empty_like(normal0)
+    score = torch.empty_like(ref)
+    changed = torch.zeros(1, dtype=torch.int64, device=dev)
+    lib = L.load()
+    stream = torch.cuda.current_stream()
+    sh = L.stream_handle()
+    a_sw, keep = dense.sweep_args(ref, mu, sd, None, srcs_k, geo, ref_cam, hyp, r, top_k, state, precision=prec)
+    pm = L.PMArgs()
+    pm.H, pm.W, pm.S = H, W, nsrc
+    pm.ref, pm.ray, pm.Cr = ref.data_ptr(), ray.data_ptr(), L.host_ptr(Cr)
+    for k in range(nsrc):
+        pm.src[k] = srcs[k].data_ptr()
+        pm.src_depth[k] = 0
+        pm.src_h[k], pm.src_w[k] = H, W
+    pm.par = L.host_ptr(par)
+    pm.depth, pm.normal, pm.score, pm.active = depth.data_ptr(), normal.data_ptr(), score.data_ptr(), active.data_ptr()
+    pm.r, pm.step, pm.top_k, pm.iters = cfg.pm_radius, cfg.pm_step, top_k, iters
+    pm.geo_w, pm.geo_tol, pm.dmin, pm.dmax = 0.5, 0.02, near, far
+    pm.seed, pm.it0, pm.changed = 12345 + rank, 0, changed.data_ptr()
+    ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in ("sweep", "pm")}
+    acc = {"sweep": 0.0, "pm": 0.0}
+    import ctypes
+
+    def step(timed: bool):
+        for t in state[:4]:
+            t.fill_(-2.0)
+        state[4].fill_(-1)
+        if timed:
+            ev["sweep"][0].record(stream)
+        L.check(lib.mvs_sweep(ctypes.addressof(a_sw), sh), "sweep")
+        if timed:
+            ev["sweep"][1].record(stream)
+        h = hyp.c()
+        L.check(lib.mvs_sweep_finalize(H, W, ctypes.addressof(h), state[0].data_ptr(), state[2].data_ptr(),
+                                       state[3].data_ptr(), state[4].data_ptr(), depth.data_ptr(), sh), "finalize")
+        if iters > 0:
+            normal.copy_(normal0)
+            score.zero_()
+            if timed:
+                ev["pm"][0].record(stream)
+            L.check(lib.mvs_pm_refine(ctypes.addressof(pm), sh), "pm_refine")
+            if timed:
+                ev["pm"][1].record(stream)
+        if timed:
+            stream.synchronize()
+            acc["sweep"] += ev["sweep"][0].elapsed_time(ev["sweep"][1])
+            if iters > 0:
+                acc["pm"] += ev["pm"][0].elapsed_time(ev["pm"][1])
+
+    setup_s = time.time() - t0
+    for _ in range(a.warmup):
+        step(False)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    # device-time of the K timed steps (events around the whole loop), plus per-kernel events
+    # measured in a second pass so that their syncs do not enter the whole-step number
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(a.steps):
+            step(False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms_total = e0.elapsed_time(e1)
+        for _ in range(a.steps):
+            step(True)
+    ms = torch.tensor([ms_total], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    ms_total = float(ms.item())
+    sweep_evals = H * W * nplanes * nsrc
+    pm_evals = H * W * iters * PM_HYPS * nsrc
+    evals = sweep_evals + pm_evals
+    value = world * evals * a.steps / (ms_total / 1e3)
+    ms_sweep = acc["sweep"] / a.steps
+    ms_pm = acc["pm"] / a.steps if iters else 0.0
+    peaks = peaks_table()
+    # sweep roofline: algorithmic bytes per evaluation (source pixel read once per plane, plus the
+    # reference statistics and the winner state once per chunk)
+    b_src = 2.0 if prec == L.PREC_FP16 else 4.0
+    bytes_per_eval = b_src + (12.0 + 20.0) / (nplanes * nsrc)
+    sweep_gbs = sweep_evals * bytes_per_eval / (ms_sweep / 1e3) / 1e9
+    traffic = read_traffic("sweep")
+    roof_sweep = {"kernel": "sweep_kernel", "bound": "hbm", "achieved": round(sweep_gbs, 1),
+                  "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sweep_gbs / peaks["hbm_gbs"], 4),
+                  "traffic": traffic, "peak_source": peaks["source"], "bytes_per_eval": round(bytes_per_eval, 4),
+                  "evals_per_s": sweep_evals / (ms_sweep / 1e3), "ms": round(ms_sweep, 3)}
+    roof_pm = None
+    if iters:
+        roof_pm = {"kernel": "pm_kernel", "bound": "fp64-issue", "evals_per_s": pm_evals / (ms_pm / 1e3),
+                   "ms": round(ms_pm, 3)}
+    dominant = "pm" if ms_pm > ms_sweep else "sweep"
+    launches = 2 + (2 * iters if iters else 0)       # sweep + finalize + 2 colour passes per iteration
+    line = {
+        "metric": "ZNCC evaluations/s (pixel x plane x view), sweep + PatchMatch",
+        "value": value / 1e9, "unit": "Gpix.plane.view/s", "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if prec == L.PREC_FP32 else "f16-storage/f32-sums",
+        "data": "synthetic seeded heightfield scene (hills + boxes, value-noise texture, nadir pinhole views)",
+        "config": {"workload": f"{cfg.name}", "width": W, "height": H, "sources": nsrc, "planes": nplanes,
+                   "window": 2 * r + 1, "top_k": top_k, "pm_iters": iters, "pm_window": 2 * cfg.pm_radius + 1,
+                   "evals_per_step": evals, "sweep_evals": sweep_evals, "pm_evals_nominal": pm_evals,
+                   "l2": "inputs larger than L2 (8 sources x 48 MB)", "parallelism": f"views x{world} (replicas)"},
+        "roofline": roof_sweep if dominant == "sweep" else dict(roof_sweep, note="pm dominates; see roofline_pm"),
+        "roofline_pm": roof_pm,
+        "phases_ms": {"sweep": round(ms_sweep, 3), "patchmatch": round(ms_pm, 3)},
+        "clocks": clocks.summary(),
+        "gpu_launches": launches * a.steps,
+        "setup_s": round(setup_s, 1),
+    }
+    if not a.no_e2e:
+        line["e2e"] = run_e2e(a, ref_h, srcs_h, geo, ref_cam, hyp, r, top_k, pm, normal0, H, W, iters, evals, world,
+                              prec)
+    if rank == 0 and not a.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(cfg, nplanes, iters, budget_s=12.0)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(a, ref_h, srcs_h, geo, ref_cam, hyp, r, top_k, pm_tmpl, normal0, H, W, iters, evals, world, prec):
+    """Same step through the public API with host buffers: pinned host -> device copies of the
+    reference and source images, window statistics, sweep, finalize, PatchMatch, and device ->
+    host copies of depth, normal and score, all inside the timed region."""
+    import ctypes
+    import torch
+    from py_ortho_b200 import _lib as L
+    from py_ortho_b200 import dense
+    dev = torch.device("cuda", torch.cuda.current_device())
+    lib = L.load()
+    stream = torch.cuda.current_stream()
+    sh = L.stream_handle()
+    h_ref = torch.from_numpy(ref_h).pin_memory()
+    h_srcs = [torch.from_numpy(s).pin_memory() for s in srcs_h]
+    d_ref = torch.empty((H, W), dtype=torch.float32, device=dev)
+    d_srcs = [torch.empty_like(d_ref) for _ in h_srcs]
+    d16 = [torch.empty((H, W), dtype=torch.float16, device=dev) for _ in h_srcs] if prec == L.PREC_FP16 else None
+    mu, sd = torch.empty_like(d_ref), torch.empty_like(d_ref)
+    state = dense.new_state(H, W, dev)
+    depth = torch.empty_like(d_ref)
+    normal = torch.empty_like(normal0)     # normal0: the job's seeded initial normals (device-resident)
+    score = torch.empty_like(d_ref)
+    h_depth = torch.empty((H, W), dtype=torch.float32).pin_memory()
+    h_normal = torch.empty((3, H, W), dtype=torch.float32).pin_memory()
+    h_score = torch.empty((H, W), dtype=torch.float32).pin_memory()
+    kern_srcs = d16 if d16 is not None else d_srcs
+    a_sw, keep = dense.sweep_args(d_ref, mu, sd, None, kern_srcs, geo, ref_cam, hyp, r, top_k, state, precision=prec)
+    pm = L.PMArgs()
+    ctypes.memmove(ctypes.addressof(pm), ctypes.addressof(pm_tmpl), ctypes.sizeof(pm))
+    pm.ref = d_ref.data_ptr()
+    for k in range(len(d_srcs)):
+        pm.src[k] = d_srcs[k].data_ptr()
+    pm.depth, pm.normal, pm.score = depth.data_ptr(), normal.data_ptr(), score.data_ptr()
+
+    def step():
+        d_ref.copy_(h_ref, non_blocking=True)
+        for d, h in zip(d_srcs, h_srcs):
+            d.copy_(h, non_blocking=True)
+        if d16 is not None:
+            for d, h16 in zip(d_srcs, d16):
+                L.check(lib.mvs_to_fp16(d.numel(), d.data_ptr(), h16.data_ptr(), sh))
+        L.check(lib.mvs_ref_stats(H, W, d_ref.data_ptr(), r, mu.data_ptr(), sd.data_ptr(), sh))
+        for t in state[:4]:
+            t.fill_(-2.0)
+        state[4].fill_(-1)
+        L.check(lib.mvs_sweep(ctypes.addressof(a_sw), sh))
+        h = hyp.c()
+        L.check(lib.mvs_sweep_finalize(H, W, ctypes.addressof(h), state[0].data_ptr(), state[2].data_ptr(),
+                                       state[3].data_ptr(), state[4].data_ptr(), depth.data_ptr(), sh))
+        if iters:
+            normal.copy_(normal0)
+            score.zero_()
+            L.check(lib.mvs_pm_refine(ctypes.addressof(pm), sh))
+        h_depth.copy_(depth, non_blocking=True)
+        h_normal.copy_(normal, non_blocking=True)
+        h_score.copy_(score, non_blocking=True)
+
+    for _ in range(max(1, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    h2d = (1 + len(h_srcs)) * H * W * 4
+    d2h = 5 * H * W * 4
+    return {"value": world * evals * a.steps / (ms / 1e3) / 1e9, "unit": "Gpix.plane.view/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "ms_per_step": ms / a.steps}
+
+
+def peaks_table():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return {"hbm_gbs": float(j["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def read_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary (profiles/), if present."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f).get(kernel)
+    return None
+
+
+# ------------------------------------------------------------------ CPU baseline (reference code)
+def cpu_baseline(cfg, nplanes, iters, budget_s: float = 12.0):
+    """The reference's own CPU kernels (oracle/_ref: _dense.sweep_hypothesis and _dense.pm_refine
+    compiled from its sources; falls back to the oracle's C restatement when the reference was
+    not built) timed on a bounded sample of the same workload with a thread pool over all host
+    cores (row bands of the view, as densify's view-level thread pool keeps every core busy).
+    Throughput in the same unit; the full-size step time is extrapolated per evaluation."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    from py_ortho_b200 import scene as S
+    R = O.reference()
+    kind = "reference" if R is not None else "port"
+    cores = os.cpu_count() or 1
+    r = cfg.radius
+    # sample: a reduced-size view with the workload's source count, window and plane spacing
+    sc = S.make_scene(cfg, seed=0, width=512, height=384)
+    ref = sc.grey(sc.ref)
+    srcs = [sc.grey(s) for s in sc.srcs]
+    H, W = ref.shape
+    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+    ray = O.rays_world((H, W), sc.ref_cam)
+    planes = S.plane_list(cfg.depth_range[0], cfg.depth_range[1], nplanes)
+    mu, sd = O.ref_stats(ref, r)
+    nb = cores
+    bands = [(max(0, (H * k) // nb - r), min(H, (H * (k + 1)) // nb + r), (H * k) // nb, (H * (k + 1)) // nb)
+             for k in range(nb)]
+    n_pl = max(1, min(nplanes, 32))
+    sel = planes[np.linspace(0, nplanes - 1, n_pl).astype(int)]
+
+    def band(b):
+        y0, y1, _, _ = b
+        st = O.init_state(y1 - y0, W)
+        rr, mm, ss, ry = (np.ascontiguousarray(x[..., y0:y1, :]) for x in (ref, mu, sd, ray))
+        for i, p in enumerate(sel):
+            inv = np.full((y1 - y0, W), p, np.float32)
+            if R is not None:
+                R._dense.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
+            else:
+                O.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
+        return (b[3] - b[2]) * W * len(sel) * len(srcs)
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(cores) as ex:
+        sweep_done = sum(ex.map(band, bands))
+    t_sweep = time.perf_counter() - t0
+    sweep_rate = sweep_done / t_sweep
+    pm_rate = None
+    if iters and R is not None:
+        ph, pw = 48, 64
+        crops = []
+        for k in range(cores):
+            y0 = (k * 37) % (H - ph)
+            x0 = (k * 53) % (W - pw)
+            crops.append((y0, x0))
+        par = np.array([c.row() for c in sc.src_cams], np.float64)
+
+        def pm_crop(c):
+            y0, x0 = c
+            rr = np.ascontiguousarray(ref[y0:y0 + ph, x0:x0 + pw])
+            ry = np.ascontiguousarray(ray[:, y0:y0 + ph, x0:x0 + pw])
+            d = np.ascontiguousarray(sc.depth_true[y0:y0 + ph, x0:x0 + pw], np.float32)
+            nrm = S.tilted_normals(ph, pw, 7)
+            scr = np.zeros((ph, pw), np.float32)
+            act = np.ones((ph, pw), np.uint8)
+            R._dense.pm_refine(rr, ry, np.asarray(sc.ref_cam.C, np.float64), srcs, [None] * len(srcs), par, d, nrm,
+                               scr, act, cfg.pm_radius, cfg.pm_step, cfg.top_k, 0.5, 0.02, 1, cfg.depth_range[0],
+                               cfg.depth_range[1], 7)
+            return ph * pw * PM_HYPS * len(srcs)
+
+        t0 = time.perf_counter()
+        with ThreadPoolExecutor(cores) as ex:
+            pm_done = sum(ex.map(pm_crop, crops))
+        pm_rate = pm_done / (time.perf_counter() - t0)
+    full_sweep = cfg.width * cfg.height * nplanes * len(srcs)
+    full_pm = cfg.width * cfg.height * iters * PM_HYPS * len(srcs)
+    t_full = full_sweep / sweep_rate + (full_pm / pm_rate if pm_rate else 0.0)
+    return {"value": (full_sweep + full_pm) / t_full / 1e9, "unit": "Gpix.plane.view/s", "cores": cores,
+            "kind": kind, "sweep_rate": sweep_rate / 1e9, "pm_rate": None if pm_rate is None else pm_rate / 1e9,
+            "sample": f"sweep: 512x384 view, {len(srcs)} sources, {len(sel)} of {nplanes} planes, "
+                      f"{len(bands)} row bands on {cores} threads; PatchMatch: {cores} 64x48 crops x 1 iteration; "
+                      f"full step extrapolated per evaluation ({t_full:.1f} s)"}
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cfg, W, H, nplanes, iters = workload(a)
+    for _ in range(a.warmup):
+        pass
+    vals = []
+    last = None
+    for _ in range(a.steps):
+        last = cpu_baseline(cfg, nplanes, iters, budget_s=10.0)
+        vals.append(last["value"])
+    v = statistics.median(vals)
+    line = {"metric": "ZNCC evaluations/s (pixel x plane x view), sweep + PatchMatch", "value": v,
+            "unit": "Gpix.plane.view/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (reference CPU)",
+            "data": "synthetic seeded heightfield scene",
+            "config": {"workload": cfg.name, "width": W, "height": H, "planes": nplanes, "pm_iters": iters},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "Gpix.plane.view/s", "cores": last["cores"], "kind": last["kind"],
+                             "sample": last["sample"]},
+            "e2e": {"value": v, "unit": "Gpix.plane.view/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

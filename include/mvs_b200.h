@@ -1,0 +1,240 @@
+/*
+ * mvs_b200.h - C ABI of the B200 multi-view-stereo depth-map engine (libmvs_b200.so).
+ *
+ * Drop-in replacement for the depth-map path of pyOrthomosaic 0.9.3: the plane sweep
+ * (`_dense.sweep_hypothesis`, `densify._sweep`) and the slanted-plane PatchMatch repair
+ * (`_dense.pm_refine`), plus the small per-view helpers that feed them (`_fast.*`).
+ *
+ * Conventions (the reference's, kept on purpose):
+ *   - the caller allocates every input and output; state arrays are updated in place;
+ *   - images are C-contiguous row-major, pixel centres at integer coordinates;
+ *   - cameras use the reference's 18-double rows (R(9, world->camera, row-major) C(3) f k1 k2 k3
+ *     cx cy) or the sweep's geo rows (Rs(9) b(3) f k1 k2 k3 cx cy, b = Rs (C_ref - C_src));
+ *   - every image/state pointer is a DEVICE pointer (cudaMalloc / torch CUDA tensor storage);
+ *     camera rows, plane lists and other small tables are HOST pointers;
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream). Work is enqueued
+ *     asynchronously; the call returns after launch (errors found at launch are returned).
+ *   - status codes map to Python exceptions in the ctypes shim: MVS_ERR_VALUE -> ValueError,
+ *     MVS_ERR_MEMORY -> MemoryError, MVS_ERR_TIMEOUT -> TimeoutError, others -> RuntimeError.
+ *     mvs_last_error() returns the message of the calling thread's last failure.
+ *
+ * No function here falls back to the CPU.
+ */
+#ifndef MVS_B200_H
+#define MVS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MVS_MAX_SOURCES 16
+#define MVS_MAX_RADIUS 7          /* window (2r+1)^2 up to 15x15 */
+#define MVS_MAX_PLANES_PER_CALL 1024
+
+typedef enum mvs_status {
+    MVS_OK = 0,
+    MVS_ERR_VALUE = 1,        /* bad shapes / arguments (reference: ValueError) */
+    MVS_ERR_MEMORY = 2,       /* device allocation failed (reference: MemoryError) */
+    MVS_ERR_CUDA = 3,         /* CUDA launch or runtime error */
+    MVS_ERR_TIMEOUT = 4,      /* a bounded device-side wait ran out */
+    MVS_ERR_UNSUPPORTED = 5   /* valid request outside what this build implements */
+} mvs_status;
+
+/* Hypothesis families of the sweep. Each yields one float32 inverse depth per pixel and
+ * hypothesis index i (0 <= i < n). */
+typedef enum mvs_hyp_kind {
+    MVS_HYP_MAPS = 0,    /* explicit maps: inv_i = maps[(i - i0) * map_stride + y * W + x]      */
+    MVS_HYP_LINEAR = 1,  /* inv_i = base + (float)i * step          (_fast.hyp_linear)          */
+    MVS_HYP_REFINE = 2,  /* inv_i = max(base + (float)(i + t0) * step, 1e-6f) (_fast.hyp_refine) */
+    MVS_HYP_PLANES = 3   /* inv_i = planes[i], constant: fronto-parallel to the reference camera;
+                            pinhole cameras only (k1 = k2 = k3 = 0); evaluated as one FP64-composed
+                            homography per (plane, source, tile) instead of per-pixel rays        */
+} mvs_hyp_kind;
+
+typedef struct mvs_hyp {
+    int32_t kind;            /* mvs_hyp_kind */
+    int32_t n;               /* hypotheses in the whole sweep (finalize: interior test)           */
+    const float* maps;       /* MAPS: device (n_maps, H, W) volume, map 0 <-> hypothesis i0       */
+    int64_t map_stride;      /* MAPS: elements between consecutive maps (0 -> H * W)              */
+    const float* base;       /* LINEAR / REFINE: device (H, W)                                    */
+    const float* step;       /* LINEAR / REFINE: device (H, W)                                    */
+    int32_t t0;              /* REFINE: offset added to i                                          */
+    int32_t pad_;
+    const float* planes;     /* PLANES: HOST array of n float32 inverse depths                    */
+} mvs_hyp;
+
+/* Storage precision of source images and warped tiles. */
+typedef enum mvs_precision {
+    MVS_PREC_FP32 = 0,   /* plain: float32 images and tiles, FP32 window sums                      */
+    MVS_PREC_FP16 = 1    /* FP16 images (src pointers are __half) and FP16 warped tiles; FP32 sums
+                            with compensated variance terms; FP64 homography and parabola          */
+} mvs_precision;
+
+typedef struct mvs_sweep_args {
+    int32_t H, W;                          /* reference image                                   */
+    const float* ref;                      /* (H, W) grey, masked pixels already 0              */
+    const float* mu;                       /* (H, W) zero-padded window mean of ref             */
+    const float* sd;                       /* (H, W) window standard deviation of ref           */
+    const float* ray;                      /* (3, H, W) world rays; NULL allowed for PLANES     */
+    int32_t n_src;                         /* 1 .. MVS_MAX_SOURCES                              */
+    int32_t precision;                     /* mvs_precision                                     */
+    const void* src[MVS_MAX_SOURCES];      /* (src_h[s], src_w[s]) images, NaN = masked         */
+    int32_t src_h[MVS_MAX_SOURCES];
+    int32_t src_w[MVS_MAX_SOURCES];
+    const double* geo;                     /* HOST (n_src, 18): Rs(9) b(3) f k1 k2 k3 cx cy     */
+    const double* ref_cam;                 /* HOST 18: R(9) C(3) f k1 k2 k3 cx cy (PLANES only) */
+    mvs_hyp hyp;
+    int32_t i0, i1;                        /* hypotheses [i0, i1) are swept by this call        */
+    int32_t r;                             /* window radius, 0 .. MVS_MAX_RADIUS                */
+    int32_t top_k;                         /* score = mean of the best top_k source NCCs        */
+    int32_t plane_chunks;                  /* 0 = automatic; else CTAs per tile along planes   */
+    int32_t pad_;
+    float* best;                           /* (H, W) in/out winner-take-all state               */
+    float* prev;
+    float* s_prev_best;
+    float* s_next_best;
+    int32_t* idx;
+} mvs_sweep_args;
+
+/* ---------------------------------------------------------------- plane sweep */
+
+/* Multi-hypothesis plane sweep: hypotheses [i0, i1) of `hyp` for every source, streaming
+ * winner-take-all state update (same per-hypothesis semantics as sweep_hypothesis, applied in
+ * hypothesis order). Replaces the hypothesis loop of densify._sweep (densify.py:336-342).
+ * Plane chunks that run in parallel are merged in hypothesis order (first index wins ties).
+ * Needs device scratch when plane_chunks > 1 (allocated stream-ordered per call). */
+mvs_status mvs_sweep(const mvs_sweep_args* args, void* stream);
+
+/* One hypothesis `i` given as an explicit inverse-depth map `inv` (H, W), ray-grid geometry
+ * with radial distortion. Replaces _dense.sweep_hypothesis (_dense.pyx:740-838); argument
+ * order and meaning as there (srcs: n_src device pointers with their shapes). */
+mvs_status mvs_sweep_hypothesis(int32_t H, int32_t W, const float* ref, const float* mu_i,
+                                const float* sd_i, int32_t n_src, const float* const* srcs,
+                                const int32_t* src_h, const int32_t* src_w, const float* ray,
+                                const double* geo, const float* inv, int32_t r, int32_t top_k,
+                                int32_t i, float* best, float* prev, float* s_prev_best,
+                                float* s_next_best, int32_t* idx, void* stream);
+
+/* Sub-hypothesis parabola and depth (camera-axis metres) from the winner-take-all state:
+ * den = spb - 2 best + snb; interior = 0 < idx < n-1 and den < -1e-6;
+ * off = clip(0.5 (spb - snb) / den, +-0.5); inv = inv_0 + (idx + off) (inv_1 - inv_0);
+ * depth = 1 / max(inv, 1e-9). Replaces densify.py:354-361 (same float32 / float64 steps). */
+mvs_status mvs_sweep_finalize(int32_t H, int32_t W, const mvs_hyp* hyp, const float* best,
+                              const float* s_prev_best, const float* s_next_best,
+                              const int32_t* idx, float* depth, void* stream);
+
+/* ---------------------------------------------------------------- per-view helpers */
+
+/* Zero-padded (2r+1)^2 window mean with float32 cumulative sums (columns, then rows), times
+ * float32(1/(2r+1)^2). Bit-identical to _fast.box_zero_mean (_fast.pyx:661-713). When
+ * `square` != 0 the input is a*a (float32), i.e. densify._box(ref * ref, r). */
+mvs_status mvs_box_zero_mean(int32_t H, int32_t W, const float* a, int32_t r, int32_t square,
+                             float* out, void* stream);
+
+/* mu = box(ref), sd = sqrt(max(box(ref*ref) - mu*mu, 1e-6)) in float32 (densify.py:327-328). */
+mvs_status mvs_ref_stats(int32_t H, int32_t W, const float* ref, int32_t r, float* mu, float* sd,
+                         void* stream);
+
+/* World ray grid (3, H, W) float32 of a camera row R(9) C(3) f k1 k2 k3 cx cy: 8 fixed-point
+ * undistortion iterations in float64, then R^T (x, y, 1). Replaces densify._rays_world with
+ * _fast.rays_grid (densify.py:288-297, _fast.pyx:145-198). */
+mvs_status mvs_rays_grid(int32_t H, int32_t W, const double* cam, float* ray, void* stream);
+
+/* out = base + (float)i * step in float32 (_fast.hyp_linear, _fast.pyx:628-641). */
+mvs_status mvs_hyp_linear(int32_t H, int32_t W, const float* base, const float* step, int64_t i,
+                          float* out, void* stream);
+
+/* out = max(iu + (float)t * ds, 1e-6f), NaN propagating (_fast.hyp_refine, _fast.pyx:644-658). */
+mvs_status mvs_hyp_refine(int32_t H, int32_t W, const float* iu, const float* ds, int64_t t,
+                          float* out, void* stream);
+
+/* uint8 RGB (h, w, 3) -> grey ((mean - 128) / 64, NaN where mask == 0) and clip(rgb+.5) uint8,
+ * with optional per-channel gain / bias (host float[3] or NULL) and mask (device uint8 or NULL).
+ * Replaces _fast.depth_view (_fast.pyx:577-624). */
+mvs_status mvs_depth_view(int32_t h, int32_t w, const uint8_t* rgb, const float* gain,
+                          const float* bias, const uint8_t* mask, float* grey, uint8_t* rgb8,
+                          void* stream);
+
+/* 2x2 mean pyramid step of `planes` stacked (h, w) float32 images: out (planes, h/2, w/2) =
+ * ((a00 + a10 + a01 + a11) * 0.25) in float32 (densify._half, densify.py:127-130; the ray
+ * pyramid at densify.py:398-403 is the same with planes = 3). */
+mvs_status mvs_half(int32_t planes, int32_t h, int32_t w, const float* in, float* out,
+                    void* stream);
+
+/* float32 -> FP16 image conversion for MVS_PREC_FP16 sources (round to nearest; NaN kept). */
+mvs_status mvs_to_fp16(int64_t n, const float* in, void* out_half, void* stream);
+
+/* ---------------------------------------------------------------- PatchMatch */
+
+typedef struct mvs_pm_args {
+    int32_t H, W;
+    const float* ref;                      /* (H, W) grey, NaN = masked                         */
+    const float* ray;                      /* (3, H, W) world rays                              */
+    const double* Cr;                      /* HOST (3) reference camera centre                  */
+    int32_t S;                             /* sources, 1 .. MVS_MAX_SOURCES (else no-op, 0)     */
+    int32_t pad_;
+    const float* src[MVS_MAX_SOURCES];     /* (src_h, src_w) float32 images                     */
+    const float* src_depth[MVS_MAX_SOURCES]; /* same shapes or NULL (no geometric term)         */
+    int32_t src_h[MVS_MAX_SOURCES];
+    int32_t src_w[MVS_MAX_SOURCES];
+    const double* par;                     /* HOST (S, 18): R(9) C(3) f k1 k2 k3 cx cy          */
+    float* depth;                          /* (H, W) in/out                                     */
+    float* normal;                         /* (3, H, W) in/out, world frame, facing the camera  */
+    float* score;                          /* (H, W) in/out                                     */
+    const uint8_t* active;                 /* (H, W) pixels to re-estimate                      */
+    int32_t r, step, top_k, iters;
+    double geo_w, geo_tol, dmin, dmax;
+    uint32_t seed;
+    int32_t it0;                           /* first iteration index (resumable jobs), usually 0 */
+    int64_t* changed;                      /* DEVICE int64 counter, incremented (may be NULL)   */
+} mvs_pm_args;
+
+/* Red-black slanted-plane PatchMatch (_dense.pm_refine, _dense.pyx:566-666). Same cost,
+ * propagation pattern, trial scales and acceptance rule; the random trials draw from a
+ * counter-based generator keyed by (seed, iteration, pixel, draw) instead of one sequential
+ * xorshift stream, so both colours of every iteration update in parallel. */
+mvs_status mvs_pm_refine(const mvs_pm_args* args, void* stream);
+
+/* The counter-based draw used by mvs_pm_refine: uniform in [0, 1) with 24-bit resolution. */
+double mvs_pm_uniform(uint32_t seed, int32_t it, int64_t pixel, int32_t draw);
+
+/* ---------------------------------------------------------------- batched sweep */
+
+typedef struct mvs_batch_job {
+    mvs_sweep_args sweep;                  /* hyp must be MVS_HYP_PLANES (one view = one job)   */
+    float* depth;                          /* (H, W) output of the fused finalize, or NULL     */
+} mvs_batch_job;
+
+typedef struct mvs_batch_tuning {
+    int32_t plane_chunk;                   /* planes per work item (0 = autotuned)             */
+    int32_t ctas_per_sm;                   /* persistent CTAs per SM (0 = occupancy maximum)  */
+} mvs_batch_tuning;
+
+typedef struct mvs_batch mvs_batch;        /* opaque: device work list, job table, graph       */
+
+/* Build a persistent batched plan over `n_jobs` views (uneven sizes, source and plane counts,
+ * radii). All device tables are allocated here; mvs_batch_run then only launches. */
+mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs,
+                            const mvs_batch_tuning* tuning, mvs_batch** out);
+/* Run every job: one persistent launch over all (job, tile, plane-chunk) work items, then the
+ * ordered chunk merge and the finalize; captured once into a CUDA graph and replayed. */
+mvs_status mvs_batch_run(mvs_batch* b, int32_t use_graph, void* stream);
+/* Number of work items and ZNCC evaluations (pixel x plane x source) in the plan. */
+mvs_status mvs_batch_stats(const mvs_batch* b, int64_t* work_items, int64_t* evals);
+void mvs_batch_destroy(mvs_batch* b);
+
+/* ---------------------------------------------------------------- misc */
+
+/* Message of this thread's last failing call ("" if none). Returns the message length. */
+size_t mvs_last_error(char* buf, size_t cap);
+/* Library version string. */
+const char* mvs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MVS_B200_H */

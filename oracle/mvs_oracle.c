@@ -1,0 +1,640 @@
+/*
+ * CPU oracle for the depth-map path - TEST INFRASTRUCTURE ONLY.
+ *
+ * Used by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl reference legs
+ * as the checker. It is never part of the product: libmvs_b200 does not link, load or call it.
+ *
+ * A plain-C restatement of the reference algorithm (pyOrthomosaic 0.9.3), written from its
+ * definitional kernels and with the same float32 / float64 rounding points, so that on the same
+ * inputs it reproduces the reference bit for bit (pinned by tests/test_oracle.py against the
+ * reference itself, compiled into oracle/_ref, and against tests/golden/ fixtures):
+ *   oracle_ncc_warp         <- _dense.ncc_warp          (_dense.pyx:13-110)
+ *   oracle_combine          <- _dense.combine           (_dense.pyx:113-144)
+ *   oracle_box_zero_mean    <- _fast.box_zero_mean      (_fast.pyx:661-713)
+ *   oracle_pm_refine        <- _dense.pm_refine         (_dense.pyx:405-666), with either the
+ *                              reference's sequential xorshift32 draws (rng = 0) or the
+ *                              counter-based draws of libmvs_b200's PatchMatch (rng = 1)
+ * plus an all-float64 variant of the sweep (oracle_sweep_fp64) used as the precision reference:
+ * every sum, NCC, score and the parabola in double, no float32 rounding anywhere.
+ *
+ * Build: oracle/Makefile (gcc -ffp-contract=off: one rounding per written operation).
+ */
+#include <math.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define EXPORT __attribute__((visibility("default")))
+
+/* ------------------------------------------------------------------ ncc_warp (_dense.pyx:13-110) */
+EXPORT int oracle_ncc_warp(int H, int W, const float* ref, const float* mu_i, const float* sd_i,
+                           const float* src, int h, int w, const float* ray, const double* Rs, const double* b,
+                           double f, double k1, double k2, double k3, double cx, double cy, const float* inv,
+                           int r, float* out, float* J, float* V, float* hs)
+{
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    const int k = 2 * r + 1;
+    const double kk = 1.0 / (k * k);
+    double* cs;
+    int y, x;
+    /* 1. warp */
+    for (y = 0; y < H; y++) {
+        for (x = 0; x < W; x++) {
+            const ptrdiff_t o = (ptrdiff_t)y * W + x;
+            double d = 1.0 / inv[o];
+            double rx = ray[o], ry = ray[HW + o], rz = ray[2 * HW + o];
+            double X = b[0] + d * ((Rs[0] * rx + Rs[1] * ry) + Rs[2] * rz);
+            double Y = b[1] + d * ((Rs[3] * rx + Rs[4] * ry) + Rs[5] * rz);
+            double Z = b[2] + d * ((Rs[6] * rx + Rs[7] * ry) + Rs[8] * rz);
+            double nx, ny, r2, dd, u, v, fx, fy, a00, a01, a10, a11, val;
+            ptrdiff_t x0, y0;
+            J[o] = 0;
+            V[o] = 0;
+            if (Z <= 1e-6) continue;
+            nx = X / Z;
+            ny = Y / Z;
+            r2 = nx * nx + ny * ny;
+            dd = f * (1 + r2 * (k1 + r2 * (k2 + r2 * k3)));
+            u = dd * nx + cx;
+            v = dd * ny + cy;
+            if (u < 0 || v < 0 || u > w - 1.001 || v > h - 1.001) continue;
+            x0 = (ptrdiff_t)u;
+            y0 = (ptrdiff_t)v;
+            fx = u - x0;
+            fy = v - y0;
+            a00 = src[y0 * w + x0];
+            a01 = src[y0 * w + x0 + 1];
+            a10 = src[(y0 + 1) * w + x0];
+            a11 = src[(y0 + 1) * w + x0 + 1];
+            val = (a00 * (1 - fx) + a01 * fx) * (1 - fy) + (a10 * (1 - fx) + a11 * fx) * fy;
+            if (isfinite(val)) {
+                J[o] = (float)val;
+                V[o] = 1;
+            }
+        }
+    }
+    /* 2. horizontal running sums (float products, double accumulators, float rows) */
+    for (y = 0; y < H; y++) {
+        const float* Jr = J + (ptrdiff_t)y * W;
+        const float* Vr = V + (ptrdiff_t)y * W;
+        const float* Ir = ref + (ptrdiff_t)y * W;
+        double sv = 0, sj = 0, sjj = 0, sij = 0;
+        for (x = 0; x < (r < W ? r : W); x++) {
+            sv += Vr[x];
+            sj += Jr[x];
+            sjj += (float)(Jr[x] * Jr[x]);
+            sij += (float)(Jr[x] * Ir[x]);
+        }
+        for (x = 0; x < W; x++) {
+            if (x + r < W) {
+                sv += Vr[x + r];
+                sj += Jr[x + r];
+                sjj += (float)(Jr[x + r] * Jr[x + r]);
+                sij += (float)(Jr[x + r] * Ir[x + r]);
+            }
+            if (x - r - 1 >= 0) {
+                sv -= Vr[x - r - 1];
+                sj -= Jr[x - r - 1];
+                sjj -= (float)(Jr[x - r - 1] * Jr[x - r - 1]);
+                sij -= (float)(Jr[x - r - 1] * Ir[x - r - 1]);
+            }
+            hs[(ptrdiff_t)y * W + x] = (float)sv;
+            hs[HW + (ptrdiff_t)y * W + x] = (float)sj;
+            hs[2 * HW + (ptrdiff_t)y * W + x] = (float)sjj;
+            hs[3 * HW + (ptrdiff_t)y * W + x] = (float)sij;
+        }
+    }
+    /* 3. vertical running sums (double) -> NCC */
+    cs = (double*)calloc((size_t)4 * W, sizeof(double));
+    if (!cs) return -1;
+    for (y = 0; y < (r < H ? r : H); y++)
+        for (x = 0; x < W; x++) {
+            int q;
+            for (q = 0; q < 4; q++) cs[q * W + x] += hs[q * HW + (ptrdiff_t)y * W + x];
+        }
+    for (y = 0; y < H; y++) {
+        for (x = 0; x < W; x++) {
+            int q;
+            double cov, mj, m2, mij, sdj, ncc;
+            if (y + r < H)
+                for (q = 0; q < 4; q++) cs[q * W + x] += hs[q * HW + (ptrdiff_t)(y + r) * W + x];
+            if (y - r - 1 >= 0)
+                for (q = 0; q < 4; q++) cs[q * W + x] -= hs[q * HW + (ptrdiff_t)(y - r - 1) * W + x];
+            cov = cs[x] * kk;
+            if (cov <= 0.9) {
+                out[(ptrdiff_t)y * W + x] = -1;
+                continue;
+            }
+            mj = cs[W + x] * kk / cov;
+            m2 = cs[2 * W + x] * kk / cov;
+            mij = cs[3 * W + x] * kk / cov;
+            sdj = m2 - mj * mj;
+            sdj = sdj > 1e-6 ? sqrt(sdj) : 1e-3;
+            ncc = (mij - mu_i[(ptrdiff_t)y * W + x] * mj) / (sd_i[(ptrdiff_t)y * W + x] * sdj);
+            out[(ptrdiff_t)y * W + x] = (float)(ncc > 1 ? 1.0 : (ncc < -1 ? -1.0 : ncc));
+        }
+    }
+    free(cs);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ combine (_dense.pyx:113-144) */
+EXPORT void oracle_combine(int n, int H, int W, const float* S, int top_k, int i, float* best, float* prev,
+                           float* s_prev_best, float* s_next_best, int* idx)
+{
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    const int kk = top_k < n ? top_k : n;
+    ptrdiff_t o;
+    for (o = 0; o < HW; o++) {
+        float buf[16], t, s;
+        int a, c;
+        for (a = 0; a < n; a++) buf[a] = S[a * HW + o];
+        for (a = 1; a < n; a++) {
+            t = buf[a];
+            c = a - 1;
+            while (c >= 0 && buf[c] < t) {
+                buf[c + 1] = buf[c];
+                c -= 1;
+            }
+            buf[c + 1] = t;
+        }
+        s = 0;
+        for (a = 0; a < kk; a++) s += buf[a];
+        s /= kk;
+        if (idx[o] == i - 1) s_next_best[o] = s;
+        if (s > best[o]) {
+            best[o] = s;
+            s_prev_best[o] = prev[o];
+            s_next_best[o] = -2;
+            idx[o] = i;
+        }
+        prev[o] = s;
+    }
+}
+
+/* One hypothesis for all sources: ncc_warp per source, then combine (the unfused definition of
+ * _dense.sweep_hypothesis). srcs: n pointers, geo: (n, 18) Rs(9) b(3) f k1 k2 k3 cx cy.
+ * If S_out is non-NULL the per-source NCC (n, H, W) is copied there. */
+EXPORT int oracle_sweep_hypothesis(int H, int W, const float* ref, const float* mu, const float* sd, int n,
+                                   const float* const* srcs, const int* src_h, const int* src_w, const float* ray,
+                                   const double* geo, const float* inv, int r, int top_k, int i, float* best,
+                                   float* prev, float* s_prev_best, float* s_next_best, int* idx, float* S_out)
+{
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    float* S = (float*)malloc(sizeof(float) * (size_t)(n * HW + 6 * HW));
+    int s, rc = 0;
+    if (!S) return -1;
+    for (s = 0; s < n && rc == 0; s++) {
+        const double* g = geo + 18 * s;
+        rc = oracle_ncc_warp(H, W, ref, mu, sd, srcs[s], src_h[s], src_w[s], ray, g, g + 9, g[12], g[13], g[14],
+                             g[15], g[16], g[17], inv, r, S + s * HW, S + n * HW, S + (n + 1) * HW, S + (n + 2) * HW);
+    }
+    if (rc == 0) {
+        oracle_combine(n, H, W, S, top_k, i, best, prev, s_prev_best, s_next_best, idx);
+        if (S_out) memcpy(S_out, S, sizeof(float) * (size_t)(n * HW));
+    }
+    free(S);
+    return rc;
+}
+
+/* ------------------------------------------------------------------ all-float64 sweep */
+/* The same sweep with no float32 rounding: warped values, window sums, NCC, top-k mean, winner
+ * state and the parabola in double; depth = 1 / max(inv0 + (idx + off) dinv, 1e-9). inv maps are
+ * given per hypothesis as double (n_hyp, H, W); ray and images as float inputs. Outputs: depth and
+ * best score (double), idx. Direct window sums (no running add/subtract). */
+EXPORT int oracle_sweep_fp64(int H, int W, const float* ref, const double* mu, const double* sd, int n,
+                             const float* const* srcs, const int* src_h, const int* src_w, const double* ray,
+                             const double* geo, const double* inv, int n_hyp, int r, int top_k, double* depth_out,
+                             double* best_out, int* idx_out)
+{
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    const int kk = top_k < n ? top_k : n;
+    double *J = (double*)malloc(sizeof(double) * HW), *S = (double*)malloc(sizeof(double) * n * HW);
+    unsigned char* V = (unsigned char*)malloc(HW);
+    double *best = (double*)malloc(sizeof(double) * HW), *prev = (double*)malloc(sizeof(double) * HW);
+    double *spb = (double*)malloc(sizeof(double) * HW), *snb = (double*)malloc(sizeof(double) * HW);
+    int* idx = idx_out;
+    int i, s, y, x;
+    ptrdiff_t o;
+    if (!J || !S || !V || !best || !prev || !spb || !snb) {
+        free(J); free(S); free(V); free(best); free(prev); free(spb); free(snb);
+        return -1;
+    }
+    for (o = 0; o < HW; o++) {
+        best[o] = prev[o] = spb[o] = snb[o] = -2.0;
+        idx[o] = -1;
+    }
+    for (i = 0; i < n_hyp; i++) {
+        const double* iv = inv + (ptrdiff_t)i * HW;
+        for (s = 0; s < n; s++) {
+            const double* g = geo + 18 * s;
+            const float* src = srcs[s];
+            const int h = src_h[s], w = src_w[s];
+            for (o = 0; o < HW; o++) {
+                double d = 1.0 / iv[o], rx = ray[o], ry = ray[HW + o], rz = ray[2 * HW + o];
+                double X = g[9] + d * (g[0] * rx + g[1] * ry + g[2] * rz);
+                double Y = g[10] + d * (g[3] * rx + g[4] * ry + g[5] * rz);
+                double Z = g[11] + d * (g[6] * rx + g[7] * ry + g[8] * rz);
+                double nx, ny, r2, dd, u, v, fx, fy, val;
+                ptrdiff_t x0, y0;
+                V[o] = 0;
+                J[o] = 0;
+                if (!(Z > 1e-6)) continue;
+                nx = X / Z;
+                ny = Y / Z;
+                r2 = nx * nx + ny * ny;
+                dd = g[12] * (1 + r2 * (g[13] + r2 * (g[14] + r2 * g[15])));
+                u = dd * nx + g[16];
+                v = dd * ny + g[17];
+                if (!(u >= 0 && v >= 0 && u <= w - 1.001 && v <= h - 1.001)) continue;
+                x0 = (ptrdiff_t)u;
+                y0 = (ptrdiff_t)v;
+                fx = u - x0;
+                fy = v - y0;
+                val = ((double)src[y0 * w + x0] * (1 - fx) + (double)src[y0 * w + x0 + 1] * fx) * (1 - fy) +
+                      ((double)src[(y0 + 1) * w + x0] * (1 - fx) + (double)src[(y0 + 1) * w + x0 + 1] * fx) * fy;
+                if (isfinite(val)) {
+                    J[o] = val;
+                    V[o] = 1;
+                }
+            }
+            for (y = 0; y < H; y++)
+                for (x = 0; x < W; x++) {
+                    double cnt = 0, sj = 0, sjj = 0, sij = 0, mj, m2, mij, var, sdj, ncc;
+                    int a, b;
+                    const int k = 2 * r + 1;
+                    for (a = -r; a <= r; a++) {
+                        const int yy = y + a;
+                        if (yy < 0 || yy >= H) continue;
+                        for (b = -r; b <= r; b++) {
+                            const int xx = x + b;
+                            const ptrdiff_t q = (ptrdiff_t)yy * W + xx;
+                            if (xx < 0 || xx >= W || !V[q]) continue;
+                            cnt += 1;
+                            sj += J[q];
+                            sjj += J[q] * J[q];
+                            sij += J[q] * (double)ref[q];
+                        }
+                    }
+                    o = (ptrdiff_t)y * W + x;
+                    if (cnt / (k * k) <= 0.9) {
+                        S[s * HW + o] = -1;
+                        continue;
+                    }
+                    mj = sj / cnt;
+                    m2 = sjj / cnt;
+                    mij = sij / cnt;
+                    var = m2 - mj * mj;
+                    sdj = var > 1e-6 ? sqrt(var) : 1e-3;
+                    ncc = (mij - mu[o] * mj) / (sd[o] * sdj);
+                    S[s * HW + o] = ncc > 1 ? 1.0 : (ncc < -1 ? -1.0 : ncc);
+                }
+        }
+        for (o = 0; o < HW; o++) {
+            double buf[16], t, sc = 0;
+            int a, c;
+            for (a = 0; a < n; a++) buf[a] = S[a * HW + o];
+            for (a = 1; a < n; a++) {
+                t = buf[a];
+                c = a - 1;
+                while (c >= 0 && buf[c] < t) {
+                    buf[c + 1] = buf[c];
+                    c--;
+                }
+                buf[c + 1] = t;
+            }
+            for (a = 0; a < kk; a++) sc += buf[a];
+            sc /= kk;
+            if (idx[o] == i - 1) snb[o] = sc;
+            if (sc > best[o]) {
+                best[o] = sc;
+                spb[o] = prev[o];
+                snb[o] = -2;
+                idx[o] = i;
+            }
+            prev[o] = sc;
+        }
+    }
+    for (o = 0; o < HW; o++) {
+        const double inv0 = inv[o], dinv = n_hyp > 1 ? inv[HW + o] - inv[o] : 0.0;
+        const double den = spb[o] - 2 * best[o] + snb[o];
+        const int in = idx[o] > 0 && idx[o] < n_hyp - 1 && den < -1e-6;
+        double off = in ? 0.5 * (spb[o] - snb[o]) / den : 0.0, iv;
+        off = off < -0.5 ? -0.5 : (off > 0.5 ? 0.5 : off);
+        iv = inv0 + (idx[o] + off) * dinv;
+        depth_out[o] = 1.0 / (iv > 1e-9 ? iv : 1e-9);
+        best_out[o] = best[o];
+    }
+    free(J); free(S); free(V); free(best); free(prev); free(spb); free(snb);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ box_zero_mean (_fast.pyx:661-713) */
+EXPORT int oracle_box_zero_mean(int H, int W, const float* a, int r, float* out)
+{
+    const int k = 2 * r + 1, PH = H + 2 * r + 1, PW = W + 2 * r + 1, R = k + 1;
+    const float scale = (float)(1.0 / (k * k));
+    float *col, *ring, *rowc;
+    int i, x, y;
+    if (H == 0 || W == 0) return 0;
+    col = (float*)malloc(sizeof(float) * W);
+    ring = (float*)malloc(sizeof(float) * (size_t)R * W);
+    rowc = (float*)malloc(sizeof(float) * PW);
+    if (!col || !ring || !rowc) {
+        free(col); free(ring); free(rowc);
+        return -1;
+    }
+    for (x = 0; x < W; x++) col[x] = 0;
+    for (i = 0; i < PH; i++) {
+        const int ay = i - (r + 1);
+        float* cur = ring + (size_t)(i % R) * W;
+        for (x = 0; x < W; x++) {
+            const float v = (ay < 0 || ay >= H) ? 0.0f : a[(ptrdiff_t)ay * W + x];
+            col[x] = (i == 0) ? v : col[x] + v;
+            cur[x] = col[x];
+        }
+        y = i - k;
+        if (y >= 0) {
+            const float* old = ring + (size_t)(y % R) * W;
+            for (x = 0; x < PW; x++) {
+                const float t = (x < r + 1 || x >= r + 1 + W) ? 0.0f : cur[x - r - 1] - old[x - r - 1];
+                rowc[x] = (x == 0) ? t : rowc[x - 1] + t;
+            }
+            for (x = 0; x < W; x++) out[(ptrdiff_t)y * W + x] = (rowc[x + k] - rowc[x]) * scale;
+        }
+    }
+    free(col); free(ring); free(rowc);
+    return 0;
+}
+
+/* ------------------------------------------------------------------ PatchMatch (_dense.pyx:405-666) */
+typedef struct {
+    const float* ref;
+    int H, W;
+    const float* ray;
+    double cr0, cr1, cr2;
+    int S;
+    const float* const* img;
+    const float* const* dep;
+    const int* iw;
+    const int* ih;
+    const double* par;
+    int r, step, top_k;
+    double geo_w, geo_tol;
+} pm_ctx;
+
+static int pm_proj(const double* p, double X, double Y, double Z, double* u, double* v, double* z)
+{
+    double dx = X - p[9], dy = Y - p[10], dz = Z - p[11];
+    double xc = p[0] * dx + p[1] * dy + p[2] * dz;
+    double yc = p[3] * dx + p[4] * dy + p[5] * dz;
+    double zc = p[6] * dx + p[7] * dy + p[8] * dz;
+    double nx, ny, r2, dd;
+    if (zc <= 1e-6) return 0;
+    nx = xc / zc;
+    ny = yc / zc;
+    r2 = nx * nx + ny * ny;
+    dd = p[12] * (1 + r2 * (p[13] + r2 * (p[14] + r2 * p[15])));
+    *u = dd * nx + p[16];
+    *v = dd * ny + p[17];
+    *z = zc;
+    return 1;
+}
+
+static double pm_bil(const float* im, int w, int h, double u, double v)
+{
+    int x0, y0;
+    double fx, fy;
+    if (!(u >= 0 && v >= 0 && u <= w - 1.001 && v <= h - 1.001)) return NAN;
+    x0 = (int)u;
+    y0 = (int)v;
+    fx = u - x0;
+    fy = v - y0;
+    return (((double)im[y0 * w + x0] * (1 - fx) + (double)im[y0 * w + x0 + 1] * fx) * (1 - fy) +
+            ((double)im[(y0 + 1) * w + x0] * (1 - fx) + (double)im[(y0 + 1) * w + x0 + 1] * fx) * fy);
+}
+
+static double pm_cost(const pm_ctx* c, int y, int x, double d, const double* n, double* ncc_out)
+{
+    const int H = c->H, W = c->W;
+    const ptrdiff_t HW = (ptrdiff_t)H * W, idx = (ptrdiff_t)y * W + x;
+    const double rpx = c->ray[idx], rpy = c->ray[HW + idx], rpz = c->ray[2 * HW + idx];
+    const double ndr = n[0] * rpx + n[1] * rpy + n[2] * rpz;
+    double sI[16], sJ[16], sII[16], sJJ[16], sIJ[16], ncc[16], num, photo, geo;
+    int cnt[16], nsamp = 0, s, a, b, kk;
+    if (ndr >= -1e-6 || d <= 0) {
+        *ncc_out = 0;
+        return 10.0;
+    }
+    num = d * ndr;
+    for (s = 0; s < c->S; s++) {
+        sI[s] = sJ[s] = sII[s] = sJJ[s] = sIJ[s] = 0;
+        cnt[s] = 0;
+    }
+    for (a = -c->r; a <= c->r; a += c->step) {
+        const int yy = y + a;
+        if (yy < 0 || yy >= H) continue;
+        for (b = -c->r; b <= c->r; b += c->step) {
+            const int xx = x + b;
+            ptrdiff_t q;
+            double I, den, t, X, Y, Z;
+            if (xx < 0 || xx >= W) continue;
+            q = (ptrdiff_t)yy * W + xx;
+            I = c->ref[q];
+            if (!isfinite(I)) continue;
+            den = n[0] * c->ray[q] + n[1] * c->ray[HW + q] + n[2] * c->ray[2 * HW + q];
+            if (den >= -1e-9) continue;
+            t = num / den;
+            X = c->cr0 + t * c->ray[q];
+            Y = c->cr1 + t * c->ray[HW + q];
+            Z = c->cr2 + t * c->ray[2 * HW + q];
+            nsamp += 1;
+            for (s = 0; s < c->S; s++) {
+                double u, v, z, J;
+                if (pm_proj(c->par + 18 * s, X, Y, Z, &u, &v, &z)) {
+                    J = pm_bil(c->img[s], c->iw[s], c->ih[s], u, v);
+                    if (isfinite(J)) {
+                        sI[s] += I;
+                        sJ[s] += J;
+                        sII[s] += I * I;
+                        sJJ[s] += J * J;
+                        sIJ[s] += I * J;
+                        cnt[s] += 1;
+                    }
+                }
+            }
+        }
+    }
+    for (s = 0; s < c->S; s++) {
+        double mi, mj, vi, vj, cv;
+        if (nsamp < 4 || cnt[s] < 0.7 * nsamp) {
+            ncc[s] = -1;
+            continue;
+        }
+        mi = sI[s] / cnt[s];
+        mj = sJ[s] / cnt[s];
+        vi = sII[s] / cnt[s] - mi * mi;
+        vj = sJJ[s] / cnt[s] - mj * mj;
+        cv = sIJ[s] / cnt[s] - mi * mj;
+        ncc[s] = (vi < 1e-8 || vj < 1e-8) ? 0 : cv / sqrt(vi * vj);
+    }
+    for (a = 1; a < c->S; a++) {
+        double tmp = ncc[a];
+        b = a - 1;
+        while (b >= 0 && ncc[b] < tmp) {
+            ncc[b + 1] = ncc[b];
+            b--;
+        }
+        ncc[b + 1] = tmp;
+    }
+    kk = c->top_k < c->S ? c->top_k : c->S;
+    photo = 0;
+    for (a = 0; a < kk; a++) photo += ncc[a];
+    photo /= kk;
+    *ncc_out = photo;
+    geo = 0;
+    if (c->geo_w > 0) {
+        const double X = c->cr0 + d * rpx, Y = c->cr1 + d * rpy, Z = c->cr2 + d * rpz;
+        int ng = 0;
+        for (s = 0; s < c->S; s++) {
+            double e = 1.0, u, v, z;
+            if (c->dep[s] == NULL) continue;
+            ng++;
+            if (pm_proj(c->par + 18 * s, X, Y, Z, &u, &v, &z)) {
+                const int ui = (int)(u + 0.5), vv = (int)(v + 0.5);
+                if (ui >= 0 && vv >= 0 && ui < c->iw[s] && vv < c->ih[s]) {
+                    const double dj = c->dep[s][(ptrdiff_t)vv * c->iw[s] + ui];
+                    if (isfinite(dj) && dj > 0) {
+                        e = fabs(z - dj) / dj / c->geo_tol;
+                        if (e > 1) e = 1;
+                    }
+                }
+            }
+            geo += e;
+        }
+        if (ng) geo /= ng;
+    }
+    return (1 - photo) + c->geo_w * geo;
+}
+
+static double rnd_xorshift(uint32_t* st)
+{
+    st[0] ^= st[0] << 13;
+    st[0] ^= st[0] >> 17;
+    st[0] ^= st[0] << 5;
+    return (st[0] & 0xFFFFFF) / 16777216.0;
+}
+
+static uint64_t mix64(uint64_t x)
+{
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ULL;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBULL;
+    x ^= x >> 31;
+    return x;
+}
+
+/* the counter-based draw of libmvs_b200's PatchMatch, restated */
+EXPORT double oracle_pm_uniform(uint32_t seed, int it, int64_t pixel, int draw)
+{
+    uint64_t x = mix64((uint64_t)seed + 0x9E3779B97F4A7C15ULL);
+    x = mix64(x ^ ((uint64_t)(uint32_t)it * 0xD1B54A32D192ED03ULL));
+    x = mix64(x ^ ((uint64_t)pixel * 0x8CB92BA72F3D8DD7ULL));
+    x = mix64(x ^ (uint64_t)(uint32_t)draw);
+    return (double)(uint32_t)(x >> 40) / 16777216.0;
+}
+
+/* rng = 0: the reference's single xorshift32 stream (seed | 1); rng = 1: counter-based draws
+ * keyed by (seed | 1, it0 + it, pixel, 4 trial + component). Returns the change count. */
+EXPORT int64_t oracle_pm_refine(int H, int W, const float* ref, const float* ray, const double* Cr, int S,
+                                const float* const* srcs, const float* const* src_depths, const int* src_h,
+                                const int* src_w, const double* par, float* depth, float* normal, float* score,
+                                const unsigned char* active, int r, int step, int top_k, double geo_w, double geo_tol,
+                                int iters, double dmin, double dmax, uint32_t seed, int rng, int it0)
+{
+    static const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
+    static const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    pm_ctx c;
+    uint32_t st = seed | 1u;
+    int64_t changed = 0;
+    int it, colour, y, x, k, tr;
+    if (S == 0 || S > 16) return 0;
+    c.ref = ref; c.H = H; c.W = W; c.ray = ray; c.cr0 = Cr[0]; c.cr1 = Cr[1]; c.cr2 = Cr[2]; c.S = S;
+    c.img = srcs; c.dep = src_depths; c.iw = src_w; c.ih = src_h; c.par = par;
+    c.r = r; c.step = step; c.top_k = top_k; c.geo_w = geo_w; c.geo_tol = geo_tol;
+    for (it = 0; it < iters; it++) {
+        const int git = it0 + it;
+        const double dd_scale = 0.05 / (git + 1), nn_scale = 0.3 / (git + 1);
+        for (colour = 0; colour < 2; colour++) {
+            for (y = 0; y < H; y++) {
+                for (x = 0; x < W; x++) {
+                    const ptrdiff_t idx = (ptrdiff_t)y * W + x;
+                    double n[3], nb[3], best, cst, ncc, sc;
+                    if (!active[idx] || (x + y) % 2 != colour) continue;
+                    n[0] = normal[idx]; n[1] = normal[HW + idx]; n[2] = normal[2 * HW + idx];
+                    if (isfinite(depth[idx])) {
+                        best = pm_cost(&c, y, x, depth[idx], n, &ncc);
+                        sc = ncc;
+                    } else {
+                        best = 1e9;
+                        sc = -1;
+                    }
+                    for (k = 0; k < 8; k++) {
+                        const int yn = y + offy[k], xn = x + offx[k];
+                        ptrdiff_t nidx;
+                        double dn, ndr, dp;
+                        if (yn < 0 || xn < 0 || yn >= H || xn >= W || !isfinite(depth[(ptrdiff_t)yn * W + xn])) continue;
+                        nidx = (ptrdiff_t)yn * W + xn;
+                        nb[0] = normal[nidx]; nb[1] = normal[HW + nidx]; nb[2] = normal[2 * HW + nidx];
+                        dn = nb[0] * ray[nidx] + nb[1] * ray[HW + nidx] + nb[2] * ray[2 * HW + nidx];
+                        ndr = nb[0] * ray[idx] + nb[1] * ray[HW + idx] + nb[2] * ray[2 * HW + idx];
+                        if (ndr >= -1e-6) continue;
+                        dp = depth[nidx] * dn / ndr;
+                        if (dp < dmin || dp > dmax) continue;
+                        cst = pm_cost(&c, y, x, dp, nb, &ncc);
+                        if (cst < best) {
+                            best = cst;
+                            sc = ncc;
+                            depth[idx] = (float)dp;
+                            normal[idx] = (float)nb[0]; normal[HW + idx] = (float)nb[1]; normal[2 * HW + idx] = (float)nb[2];
+                            changed++;
+                        }
+                    }
+                    if (isfinite(depth[idx])) {
+                        for (tr = 0; tr < 2; tr++) {
+                            double u0, u1, u2, u3, dp, nn;
+                            if (rng == 0) {
+                                u0 = rnd_xorshift(&st); u1 = rnd_xorshift(&st); u2 = rnd_xorshift(&st); u3 = rnd_xorshift(&st);
+                            } else {
+                                u0 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 0);
+                                u1 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 1);
+                                u2 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 2);
+                                u3 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 3);
+                            }
+                            dp = depth[idx] * (1 + dd_scale * (2 * u0 - 1));
+                            nb[0] = normal[idx] + nn_scale * (2 * u1 - 1);
+                            nb[1] = normal[HW + idx] + nn_scale * (2 * u2 - 1);
+                            nb[2] = normal[2 * HW + idx] + nn_scale * (2 * u3 - 1);
+                            nn = sqrt(nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]);
+                            if (nn < 1e-9 || dp < dmin || dp > dmax) continue;
+                            nb[0] /= nn; nb[1] /= nn; nb[2] /= nn;
+                            cst = pm_cost(&c, y, x, dp, nb, &ncc);
+                            if (cst < best) {
+                                best = cst;
+                                sc = ncc;
+                                depth[idx] = (float)dp;
+                                normal[idx] = (float)nb[0]; normal[HW + idx] = (float)nb[1]; normal[2 * HW + idx] = (float)nb[2];
+                                changed++;
+                            }
+                        }
+                    }
+                    score[idx] = (float)sc;
+                }
+            }
+        }
+    }
+    return changed;
+}

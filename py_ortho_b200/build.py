@@ -1,0 +1,88 @@
+"""Builds libmvs_b200.so (sm_100a) in-tree with nvcc.
+
+Usage: ``python -m py_ortho_b200.build [--force] [--verbose]``. Objects go to
+``py_ortho_b200/_build/``; the shared library to ``py_ortho_b200/libmvs_b200.so``.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+BUILD = os.path.join(HERE, "_build")
+LIB = os.path.join(HERE, "libmvs_b200.so")
+INCLUDE = os.path.join(os.path.dirname(HERE), "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
+          "--expt-relaxed-constexpr", "-I", INCLUDE]
+# per-file extra flags: PatchMatch is evaluated without contraction (float64, one rounding per op)
+EXTRA = {
+    "patchmatch.cu": ["-fmad=false"],
+}
+SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu"]
+
+
+def nvcc() -> str:
+    p = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(p):
+        raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libmvs_b200")
+    return p
+
+
+def _stale(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
+    headers.append(os.path.join(INCLUDE, "mvs_b200.h"))
+    objs = []
+    cc = nvcc()
+    for src in SOURCES:
+        path = os.path.join(CSRC, src)
+        if not os.path.exists(path):
+            continue
+        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        objs.append(obj)
+        if force or ptxas_info or _stale(obj, [path] + headers):
+            cmd = [cc, "-c", path, "-o", obj] + ARCH + COMMON + EXTRA.get(src, [])
+            if ptxas_info:
+                cmd += ["-Xptxas", "-v"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+            if ptxas_info or verbose:
+                sys.stdout.write(r.stdout + r.stderr)
+    if force or _stale(LIB, objs):
+        cmd = [cc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+    return LIB
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--verbose", action="store_true")
+    ap.add_argument("--ptxas-info", action="store_true", help="print registers / spills per kernel")
+    a = ap.parse_args(argv)
+    print(build(a.force, a.verbose, a.ptxas_info))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -1,0 +1,298 @@
+// Batched plane sweep: many reference views of uneven size, source count, plane count and
+// window radius in ONE persistent launch.
+//
+// The plan is a device work list of (job, tile_x, tile_y, plane-chunk) items ordered by cost,
+// largest first (longest-processing-time order). Persistent CTAs (a multiple of the SM count)
+// take items with one atomicAdd each, so no CTA waits on another and uneven jobs balance. A
+// job's result does not depend on what else is in the batch: its per-pixel reduction order is
+// fixed by hypothesis index (chunk records are merged in hypothesis order afterwards).
+// run = [reset counter] -> [persistent sweep] -> [ordered chunk merge + parabola finalize],
+// captured once into a CUDA graph and replayed.
+#include <vector>
+#include <algorithm>
+
+#include "sweep_tile.cuh"
+
+namespace mvs {
+
+struct JobFin {                        // per-job table of the merge / finalize pass
+    long long block0;                  // first block of this job in the finalize grid
+    long long HW;
+    int nchunks, ppc, i0, i1, n;
+    float p0, p1;
+    const float* rec;
+    float* best;
+    float* prev;
+    float* spb;
+    float* snb;
+    int* idx;
+    float* depth;
+};
+
+template <int RMAX, int KMAX, bool F16>
+__global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restrict__ jobs, const int4* __restrict__ items,
+                                                      int n_items, int* counter) {
+    extern __shared__ float4 smem4[];
+    __shared__ int s_item;
+    float* smem = reinterpret_cast<float*>(smem4);
+    for (;;) {
+        __syncthreads();                   // everyone has read the previous s_item
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        if (it >= n_items) break;
+        const int4 w = items[it];
+        const SweepParams& p = jobs[w.x];
+        const int pa = p.i0 + w.w * p.ppc;
+        const int pb = min(p.i1, pa + p.ppc);
+        sweep_tile<RMAX, true, KMAX, true, F16>(p, p.r, w.y * TW, w.z * TH, pa, pb, p.rec ? w.w : -1, smem);
+    }
+}
+
+__global__ void batch_finalize_kernel(const JobFin* __restrict__ jobs, int n_jobs) {
+    // locate the job of this block (jobs are few; binary search over block0)
+    int lo = 0, hi = n_jobs - 1;
+    const long long blk = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (jobs[mid].block0 <= blk) lo = mid; else hi = mid - 1;
+    }
+    const JobFin& j = jobs[lo];
+    const long long o = (blk - j.block0) * blockDim.x + threadIdx.x;
+    if (o >= j.HW) return;
+    float B, P, SP, SN;
+    int I;
+    if (j.rec) {
+        B = -2.f; P = -2.f; SP = -2.f; SN = -2.f; I = -1;
+        merge_pixel(o, j.HW, j.nchunks, j.i0, j.i1, j.ppc, j.rec, B, P, SP, SN, I);
+        j.best[o] = B;
+        j.prev[o] = P;
+        j.spb[o] = SP;
+        j.snb[o] = SN;
+        j.idx[o] = I;
+    } else {
+        B = j.best[o]; SP = j.spb[o]; SN = j.snb[o]; I = j.idx[o];
+    }
+    if (j.depth) j.depth[o] = finalize_pixel(j.p0, j.p1, j.n, B, SP, SN, I);
+}
+
+template <int RMAX, int KMAX, bool F16>
+static mvs_status batch_attr(int* max_ctas_per_sm) {
+    auto kern = batch_kernel<RMAX, KMAX, F16>;
+    const size_t smem = Geom<RMAX>::smem_bytes();
+    MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "batch: smem attribute");
+    MVS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_ctas_per_sm, kern, NT, smem), "batch: occupancy");
+    return MVS_OK;
+}
+
+template <int RMAX, int KMAX, bool F16>
+static void batch_launch(dim3 grid, cudaStream_t st, const SweepParams* jobs, const int4* items, int n, int* counter) {
+    batch_kernel<RMAX, KMAX, F16><<<grid, NT, Geom<RMAX>::smem_bytes(), st>>>(jobs, items, n, counter);
+}
+
+}  // namespace mvs
+
+using namespace mvs;
+
+struct mvs_batch {
+    int n_jobs = 0;
+    int rmax = 3, kmax = 2;
+    bool f16 = false;
+    int grid = 0;
+    int n_items = 0;
+    long long evals = 0;
+    long long fin_blocks = 0;
+    SweepParams* d_params = nullptr;
+    int4* d_items = nullptr;
+    int* d_counter = nullptr;
+    float* d_rec = nullptr;
+    JobFin* d_fin = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+static mvs_status batch_enqueue(mvs_batch* b, cudaStream_t st) {
+    MVS_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st), "batch: reset counter");
+    const dim3 grid(b->grid);
+    if (b->rmax <= 3) {
+        if (b->kmax <= 2) {
+            if (b->f16) batch_launch<3, 2, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+            else batch_launch<3, 2, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+        } else {
+            if (b->f16) batch_launch<3, 8, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+            else batch_launch<3, 8, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+        }
+    } else {
+        if (b->kmax <= 2) {
+            if (b->f16) batch_launch<7, 2, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+            else batch_launch<7, 2, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+        } else {
+            if (b->f16) batch_launch<7, 8, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+            else batch_launch<7, 8, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
+        }
+    }
+    MVS_TRY(check_launch("batch persistent kernel"));
+    batch_finalize_kernel<<<(unsigned)b->fin_blocks, 256, 0, st>>>(b->d_fin, b->n_jobs);
+    return check_launch("batch finalize kernel");
+}
+
+static void batch_free(mvs_batch* b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    cudaFree(b->d_params);
+    cudaFree(b->d_items);
+    cudaFree(b->d_counter);
+    cudaFree(b->d_rec);
+    cudaFree(b->d_fin);
+    delete b;
+}
+
+extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs, const mvs_batch_tuning* tuning,
+                                       mvs_batch** out) {
+    clear_error();
+    if (!out) return fail(MVS_ERR_VALUE, "batch: null output handle");
+    *out = nullptr;
+    if (!jobs || n_jobs < 1) return fail(MVS_ERR_VALUE, "batch: needs at least one job");
+    const int pc_req = tuning ? tuning->plane_chunk : 0;
+    const int cps_req = tuning ? tuning->ctas_per_sm : 0;
+    if (pc_req < 0 || cps_req < 0) return fail(MVS_ERR_VALUE, "batch: negative tuning value");
+    std::vector<SweepParams> params(n_jobs);
+    std::vector<JobFin> fin(n_jobs);
+    std::vector<int4> items;
+    std::vector<long long> cost;
+    long long rec_floats = 0;
+    mvs_batch* b = new mvs_batch();
+    b->n_jobs = n_jobs;
+    b->f16 = jobs[0].sweep.precision == MVS_PREC_FP16;
+    int rmax = 0, kmax = 2;
+    std::vector<long long> rec_off(n_jobs, -1);
+    for (int j = 0; j < n_jobs; ++j) {
+        const mvs_sweep_args* a = &jobs[j].sweep;
+        mvs_status st = validate_sweep(a);
+        if (st != MVS_OK) { batch_free(b); return st; }
+        if (a->hyp.kind != MVS_HYP_PLANES) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d must use MVS_HYP_PLANES", j); }
+        if ((a->precision == MVS_PREC_FP16) != b->f16) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: all jobs need the same precision"); }
+        if (a->i1 - a->i0 > MVS_MAX_PLANES_PER_CALL) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d has more than %d planes", j, MVS_MAX_PLANES_PER_CALL); }
+        if (a->H == 0 || a->W == 0 || a->i1 == a->i0) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d is empty", j); }
+        SweepParams& p = params[j];
+        st = fill_params(a, p);
+        if (st != MVS_OK) { batch_free(b); return st; }
+        kmax = std::max(kmax, pick_kmax(p));
+        rmax = std::max(rmax, a->r);
+        const int n = a->i1 - a->i0;
+        for (int k = 0; k < n; ++k) p.planes[k] = a->hyp.planes[a->i0 + k];
+        p.i0 = a->i0;
+        p.i1 = a->i1;
+        p.r = a->r;
+        p.fresh = 1;
+        const int pc = pc_req > 0 ? std::min(pc_req, n) : n;
+        p.ppc = pc;
+        p.nchunks = (n + pc - 1) / pc;
+        const int tx = (a->W + TW - 1) / TW, ty = (a->H + TH - 1) / TH;
+        if (p.nchunks > 1) {
+            rec_off[j] = rec_floats;
+            rec_floats += (long long)6 * p.nchunks * a->H * a->W;
+        }
+        for (int ch = 0; ch < p.nchunks; ++ch) {
+            const int planes = std::min(pc, n - ch * pc);
+            for (int y = 0; y < ty; ++y)
+                for (int x = 0; x < tx; ++x) {
+                    items.push_back(make_int4(j, x, y, ch));
+                    cost.push_back((long long)planes * a->n_src * (TW + 2 * a->r) * (TH + 2 * a->r));
+                }
+        }
+        b->evals += (long long)a->H * a->W * n * a->n_src;
+        JobFin& f = fin[j];
+        f.HW = (long long)a->H * a->W;
+        f.nchunks = p.nchunks; f.ppc = pc; f.i0 = a->i0; f.i1 = a->i1; f.n = a->hyp.n;
+        f.p0 = a->hyp.planes[0];
+        f.p1 = a->hyp.n > 1 ? a->hyp.planes[1] : f.p0;
+        f.best = a->best; f.prev = a->prev; f.spb = a->s_prev_best; f.snb = a->s_next_best; f.idx = a->idx;
+        f.depth = jobs[j].depth;
+    }
+    b->rmax = rmax <= 3 ? 3 : 7;
+    b->kmax = kmax;
+    // largest items first
+    std::vector<int> order(items.size());
+    for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<int4> sorted(items.size());
+    for (size_t i = 0; i < order.size(); ++i) sorted[i] = items[order[i]];
+    b->n_items = (int)sorted.size();
+
+    int max_cps = 0;
+    mvs_status st = MVS_OK;
+    if (b->rmax <= 3) st = b->kmax <= 2 ? (b->f16 ? batch_attr<3, 2, true>(&max_cps) : batch_attr<3, 2, false>(&max_cps))
+                                        : (b->f16 ? batch_attr<3, 8, true>(&max_cps) : batch_attr<3, 8, false>(&max_cps));
+    else st = b->kmax <= 2 ? (b->f16 ? batch_attr<7, 2, true>(&max_cps) : batch_attr<7, 2, false>(&max_cps))
+                           : (b->f16 ? batch_attr<7, 8, true>(&max_cps) : batch_attr<7, 8, false>(&max_cps));
+    if (st != MVS_OK) { batch_free(b); return st; }
+    if (max_cps < 1) { batch_free(b); return fail(MVS_ERR_CUDA, "batch: kernel does not fit on an SM"); }
+    const int cps = cps_req > 0 ? std::min(cps_req, max_cps) : max_cps;
+    b->grid = num_sms() * cps;
+
+#define BATCH_ALLOC(ptr, bytes, what)                                                       \
+    do {                                                                                    \
+        cudaError_t e__ = cudaMalloc((void**)&(ptr), (bytes));                              \
+        if (e__ != cudaSuccess) { batch_free(b); return fail(MVS_ERR_MEMORY, "batch: %s: %s", what, cudaGetErrorString(e__)); } \
+    } while (0)
+    BATCH_ALLOC(b->d_params, sizeof(SweepParams) * n_jobs, "job table");
+    BATCH_ALLOC(b->d_items, sizeof(int4) * sorted.size(), "work list");
+    BATCH_ALLOC(b->d_counter, sizeof(int), "counter");
+    if (rec_floats) BATCH_ALLOC(b->d_rec, sizeof(float) * rec_floats, "chunk records");
+    BATCH_ALLOC(b->d_fin, sizeof(JobFin) * n_jobs, "finalize table");
+#undef BATCH_ALLOC
+    long long blocks = 0;
+    for (int j = 0; j < n_jobs; ++j) {
+        if (rec_off[j] >= 0) {
+            params[j].rec = b->d_rec + rec_off[j];
+            fin[j].rec = params[j].rec;
+        } else {
+            params[j].rec = nullptr;
+            fin[j].rec = nullptr;
+        }
+        fin[j].block0 = blocks;
+        blocks += (fin[j].HW + 255) / 256;
+    }
+    b->fin_blocks = blocks;
+    cudaError_t e = cudaMemcpy(b->d_params, params.data(), sizeof(SweepParams) * n_jobs, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_items, sorted.data(), sizeof(int4) * sorted.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_fin, fin.data(), sizeof(JobFin) * n_jobs, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { batch_free(b); return fail(MVS_ERR_CUDA, "batch: upload: %s", cudaGetErrorString(e)); }
+    *out = b;
+    return MVS_OK;
+}
+
+extern "C" mvs_status mvs_batch_run(mvs_batch* b, int32_t use_graph, void* stream) {
+    clear_error();
+    if (!b) return fail(MVS_ERR_VALUE, "batch: null handle");
+    cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : b->own_stream;
+    if (!use_graph) return batch_enqueue(b, st);
+    if (!b->exec) {
+        // capture on the private stream (capture is not possible on the legacy default stream)
+        MVS_CUDA(cudaStreamBeginCapture(b->own_stream, cudaStreamCaptureModeThreadLocal), "batch: begin capture");
+        mvs_status s = batch_enqueue(b, b->own_stream);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(b->own_stream, &g);
+        if (s != MVS_OK) { if (g) cudaGraphDestroy(g); return s; }
+        if (e != cudaSuccess) return fail(MVS_ERR_CUDA, "batch: end capture: %s", cudaGetErrorString(e));
+        b->graph = g;
+        MVS_CUDA(cudaGraphInstantiate(&b->exec, g, 0), "batch: instantiate graph");
+    }
+    MVS_CUDA(cudaGraphLaunch(b->exec, st), "batch: graph launch");
+    return MVS_OK;
+}
+
+extern "C" mvs_status mvs_batch_stats(const mvs_batch* b, int64_t* work_items, int64_t* evals) {
+    clear_error();
+    if (!b) return fail(MVS_ERR_VALUE, "batch: null handle");
+    if (work_items) *work_items = b->n_items;
+    if (evals) *evals = b->evals;
+    return MVS_OK;
+}
+
+extern "C" void mvs_batch_destroy(mvs_batch* b) { batch_free(b); }

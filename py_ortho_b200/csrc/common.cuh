@@ -1,0 +1,64 @@
+// Shared helpers of libmvs_b200: status / last-error plumbing and small device utilities.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <stdarg.h>
+#include <string.h>
+
+#include "../../include/mvs_b200.h"
+
+namespace mvs {
+
+// Thread-local message of the last failing call (the reference raises with a message; the
+// ctypes shim reads this and raises the matching Python exception).
+void set_error(const char* fmt, ...);
+void clear_error();
+
+inline mvs_status fail(mvs_status st, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    set_error("%s", buf);
+    return st;
+}
+
+inline mvs_status check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        return fail(e == cudaErrorMemoryAllocation ? MVS_ERR_MEMORY : MVS_ERR_CUDA,
+                    "%s: %s", what, cudaGetErrorString(e));
+    }
+    return MVS_OK;
+}
+
+#define MVS_TRY(expr)                        \
+    do {                                     \
+        mvs_status st__ = (expr);            \
+        if (st__ != MVS_OK) return st__;     \
+    } while (0)
+
+#define MVS_CUDA(expr, what)                                                              \
+    do {                                                                                  \
+        cudaError_t e__ = (expr);                                                         \
+        if (e__ != cudaSuccess)                                                           \
+            return ::mvs::fail(e__ == cudaErrorMemoryAllocation ? MVS_ERR_MEMORY             \
+                                                                : MVS_ERR_CUDA,           \
+                               "%s: %s", what, cudaGetErrorString(e__));                  \
+    } while (0)
+
+inline int num_sms() {
+    int dev = 0, n = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+// NaN-propagating max with a float32 floor (np.maximum semantics).
+__device__ __forceinline__ float max_nan(float v, float lo) { return (v >= lo || v != v) ? v : lo; }
+__device__ __forceinline__ double max_nan(double v, double lo) { return (v >= lo || v != v) ? v : lo; }
+
+}  // namespace mvs

@@ -1,0 +1,257 @@
+"""Generates the golden fixtures in tests/golden/ by running the REFERENCE implementation
+(pyOrthomosaic 0.9.3: its own densify.py with its own _dense / _fast kernels compiled from
+source into oracle/_ref) on seeded inputs.
+
+Run where the reference tree exists:  make -C oracle ref && python tests/golden/make_golden.py
+The fixtures travel with the repository; nothing at test time needs the reference.
+
+Fixtures (each .npz holds the inputs and the reference outputs):
+  sweep_cases.npz  - _dense.sweep_hypothesis over several hypotheses for shapes of the
+                     reference's own parity tests (H, W, n, r, top_k, n_hyp), with 2 % NaN source
+                     pixels, +-3 px source size jitter, inv = inf and inv < 0 injected; final
+                     winner state and every hypothesis' top-k score (the `prev` array after each
+                     call, _sweep.h:212); plus one flat-image tie case
+  sweep_e2e.npz    - densify._sweep end to end (lazy hypotheses, parabola) -> depth, best, sd
+  scene_small.npz  - a seeded synthetic nadir scene (uint8 images, pinhole cameras, constant
+                     inverse-depth planes) through densify._sweep -> depth, best, sd and the
+                     best-to-second hypothesis score gap
+  helpers.npz      - _fast.box_zero_mean, hyp_linear, hyp_refine, depth_view, densify._rays_world
+  pm_case.npz      - _dense.pm_refine (the reference's xorshift draws) on a small case
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import refpkg  # noqa: E402
+from oracle import oracle as O  # noqa: E402
+
+SHAPES = [(37, 53, 4, 5, 2, 9), (64, 48, 1, 3, 2, 5), (11, 9, 3, 5, 2, 4), (5, 4, 2, 5, 1, 3),
+          (30, 31, 5, 2, 3, 6), (2, 40, 2, 1, 2, 3), (40, 3, 4, 4, 4, 3), (48, 64, 8, 3, 2, 7),
+          (33, 47, 16, 2, 9, 4)]
+
+
+def rotation(rng, tilt):
+    """Rotation near a nadir view (180 deg about x) with a random tilt (Rodrigues)."""
+    w = rng.normal(0, tilt, 3) + np.array([np.pi, 0, 0])
+    th = np.linalg.norm(w)
+    k = w / th
+    K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+
+
+def random_case(rng, H, W, n, r, nhyp, nan_frac=0.02):
+    ref = rng.normal(0, 1, (H, W)).astype(np.float32)
+    srcs = []
+    for _ in range(n):
+        h = max(H + int(rng.integers(-3, 4)), 2)
+        w = max(W + int(rng.integers(-3, 4)), 2)
+        s = rng.normal(0, 1, (h, w)).astype(np.float32)
+        s[rng.random(s.shape) < nan_frac] = np.nan
+        srcs.append(np.ascontiguousarray(s))
+    ray = rng.normal(0, 0.3, (3, H, W)).astype(np.float32)
+    ray[2] = 1.0 + rng.normal(0, 0.01, (H, W)).astype(np.float32)
+    geo = []
+    for _ in range(n):
+        Rs = rotation(rng, 0.05) @ rotation(rng, 0.0).T
+        b = rng.normal(0, 0.5, 3)
+        f = float(rng.uniform(0.8, 1.2) * W)
+        geo.append(np.r_[Rs.ravel(), b, [f, rng.normal(0, 0.05), rng.normal(0, 0.01), rng.normal(0, 0.003),
+                                         (W - 1) / 2 + rng.normal(0, 2), (H - 1) / 2 + rng.normal(0, 2)]])
+    base = rng.uniform(0.02, 0.2, (H, W)).astype(np.float32)
+    step = rng.uniform(1e-4, 5e-3, (H, W)).astype(np.float32)
+    hyps = np.stack([(base + i * step).astype(np.float32) for i in range(nhyp)])
+    if nhyp > 2:
+        hyps[1, 0, 0] = np.inf
+        hyps[2, -1, -1] = -0.01
+    return ref, srcs, ray, np.array(geo, np.float64), hyps
+
+
+def run_reference_sweep(R, ref, srcs, ray, geo, hyps, r, top_k):
+    H, W = ref.shape
+    mu = R._fast.box_zero_mean(ref, r)
+    sd = np.sqrt(np.maximum(R._fast.box_zero_mean(np.ascontiguousarray(ref * ref), r) - mu * mu, 1e-6)).astype(
+        np.float32)
+    best, prev, spb, snb, idx = O.init_state(H, W)
+    scores = np.empty((len(hyps), H, W), np.float32)
+    for i, inv in enumerate(hyps):
+        R._dense.sweep_hypothesis(ref, mu, sd, srcs, ray, geo, np.ascontiguousarray(inv), r, top_k, i, best, prev,
+                                  spb, snb, idx)
+        scores[i] = prev
+    return mu, sd, best, prev, spb, snb, idx, scores
+
+
+def sweep_cases(R):
+    rng = np.random.default_rng(7)
+    out = {}
+    for k, (H, W, n, r, top_k, nh) in enumerate(SHAPES):
+        ref, srcs, ray, geo, hyps = random_case(rng, H, W, n, r, nh)
+        mu, sd, best, prev, spb, snb, idx, scores = run_reference_sweep(R, ref, srcs, ray, geo, hyps, r, top_k)
+        p = f"c{k}_"
+        out.update({p + "meta": np.array([H, W, n, r, top_k, nh]), p + "ref": ref, p + "ray": ray, p + "geo": geo,
+                    p + "hyps": hyps, p + "mu": mu, p + "sd": sd, p + "best": best, p + "prev": prev,
+                    p + "spb": spb, p + "snb": snb, p + "idx": idx, p + "scores": scores})
+        for j, s in enumerate(srcs):
+            out[p + f"src{j}"] = s
+    # flat sources: equal scores everywhere, ties keep the first hypothesis
+    ref, srcs, ray, geo, hyps = random_case(rng, 20, 24, 3, 2, 5, 0.0)
+    flat = [np.ones_like(s) for s in srcs]
+    mu, sd, best, prev, spb, snb, idx, scores = run_reference_sweep(R, ref, flat, ray, geo, hyps, 2, 2)
+    k = len(SHAPES)
+    p = f"c{k}_"
+    out.update({p + "meta": np.array([20, 24, 3, 2, 2, 5]), p + "ref": ref, p + "ray": ray, p + "geo": geo,
+                p + "hyps": hyps, p + "mu": mu, p + "sd": sd, p + "best": best, p + "prev": prev, p + "spb": spb,
+                p + "snb": snb, p + "idx": idx, p + "scores": scores})
+    for j, s in enumerate(flat):
+        out[p + f"src{j}"] = s
+    out["ncases"] = np.array(k + 1)
+    np.savez_compressed(os.path.join(HERE, "sweep_cases.npz"), **out)
+
+
+class _Cam:
+    def __init__(self, R, C, f, k1, k2, k3, cx, cy, w=0, h=0):
+        self.R, self.C = np.asarray(R, np.float64), np.asarray(C, np.float64)
+        self.f, self.k1, self.k2, self.k3, self.cx, self.cy, self.w, self.h = f, k1, k2, k3, cx, cy, w, h
+
+
+def sweep_e2e(D):
+    rng = np.random.default_rng(3)
+    H, W = 45, 61
+    ref, srcs, ray, geo, hyps = random_case(rng, H, W, 4, 5, 19)
+    cam_r = _Cam(np.eye(3), np.zeros(3), float(W), 0.0, 0.0, 0.0, W / 2, H / 2)
+    cams_s = []
+    for g in geo:
+        Rs = g[:9].reshape(3, 3)
+        Cs = -Rs.T @ g[9:12]                   # so that Rs (C_ref - C_src) == b
+        cams_s.append(_Cam(Rs, Cs, g[12], g[13], g[14], g[15], g[16], g[17]))
+    opt = D.DepthOptions()
+    opt.window = 5
+    lazy = D._Hypotheses(lambda i: hyps[i].copy(), len(hyps))
+    depth, best, sd = D._sweep(ref, cam_r, srcs, cams_s, lazy, opt, ray)
+    out = {"ref": ref, "ray": ray, "geo": geo, "hyps": hyps, "depth": depth, "best": best, "sd": sd,
+           "meta": np.array([H, W, 4, 5, 2, 19])}
+    for j, s in enumerate(srcs):
+        out[f"src{j}"] = s
+    np.savez_compressed(os.path.join(HERE, "sweep_e2e.npz"), **out)
+
+
+def scene_small(D):
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c1", seed=3, width=160, height=120)
+    planes = S.plane_list(35.0, 55.0, 32)
+    ref = sc.grey(sc.ref)
+    srcs = [sc.grey(s) for s in sc.srcs]
+
+    def cam(c):
+        return _Cam(c.R, c.C, c.f, 0.0, 0.0, 0.0, c.cx, c.cy, c.w, c.h)
+
+    cam_r = cam(sc.ref_cam)
+    cams_s = [cam(c) for c in sc.src_cams]
+    H, W = ref.shape
+    opt = D.DepthOptions()
+    opt.window = 2
+    opt.top_k = 2
+    ray = D._rays_world(ref.shape, cam_r)
+    hyps = D._Hypotheses(lambda i: np.full((H, W), planes[i], np.float32), len(planes))
+    depth, best, sd = D._sweep(ref, cam_r, srcs, cams_s, hyps, opt, ray)
+    geo = O.geo_rows(cam_r, cams_s)
+    R = O.reference()
+    *_, scores = run_reference_sweep(R, ref, srcs, ray, geo, np.stack([hyps[i] for i in range(len(planes))]), 2, 2)
+    srt = np.sort(scores, axis=0)
+    gap = (srt[-1] - srt[-2]).astype(np.float32)          # best minus second-best hypothesis score
+    out = {"ref_u8": sc.ref, "planes": planes, "ray": ray, "geo": geo, "depth": depth, "best": best, "sd": sd,
+           "gap": gap, "ref_cam": np.r_[cam_r.R.ravel(), cam_r.C, [cam_r.f, 0, 0, 0, cam_r.cx, cam_r.cy]],
+           "meta": np.array([H, W, len(srcs), 2, 2, len(planes)]), "depth_true": sc.depth_true}
+    for j, s in enumerate(sc.srcs):
+        out[f"src{j}_u8"] = s
+    np.savez_compressed(os.path.join(HERE, "scene_small.npz"), **out)
+
+
+def helpers(D, R):
+    rng = np.random.default_rng(14)
+    out = {}
+    a = rng.normal(0, 1, (37, 53)).astype(np.float32)
+    a[a > 1.5] = -0.0
+    out["box_in"] = a
+    for r in (0, 1, 2, 5, 7):
+        out[f"box_r{r}"] = R._fast.box_zero_mean(a, r)
+        out[f"box_sq_r{r}"] = R._fast.box_zero_mean(np.ascontiguousarray(a * a), r)
+    base = rng.uniform(0.01, 0.05, (37, 53)).astype(np.float32)
+    step = rng.uniform(1e-5, 1e-3, (37, 53)).astype(np.float32)
+    out["hyp_base"], out["hyp_step"] = base, step
+    for i in (0, 1, 7, 191):
+        out[f"hyp_linear_{i}"] = R._fast.hyp_linear(base, step, i)
+    iu = rng.uniform(-1e-3, 0.05, (37, 53)).astype(np.float32)
+    iu[0, 0] = np.nan
+    out["hyp_iu"] = iu
+    for t in (-3, -1, 0, 2, 3):
+        out[f"hyp_refine_{t + 3}"] = R._fast.hyp_refine(iu, step, t)
+    rgb = rng.integers(0, 256, (29, 41, 3)).astype(np.uint8)
+    m = rng.random((29, 41)) < 0.7
+    out["dv_rgb"], out["dv_mask"] = rgb, m
+    out["dv_gain"], out["dv_bias"] = np.array([1.07, 0.93, 1.21]), np.array([-3.5, 2.25, 0.0])
+    g1, r1 = R._fast.depth_view(rgb, (1.07, 0.93, 1.21), (-3.5, 2.25, 0.0), m)
+    g0, r0 = R._fast.depth_view(rgb, None, None, None)
+    out["dv_grey"], out["dv_rgb8"], out["dv_grey0"], out["dv_rgb80"] = g1, r1, g0, r0
+    cam = D._Cam(rotation(rng, 0.1), np.array([1.0, -2.0, 50.0]), 1000.0, -0.05, 0.01, 511.3, 383.7, 1024, 768,
+                 0.003)
+    out["rays_cam"] = np.r_[cam.R.ravel(), cam.C, [cam.f, cam.k1, cam.k2, cam.k3, cam.cx, cam.cy]]
+    out["rays"] = D._rays_world((96, 128), cam)
+    half_in = rng.normal(0, 1, (3, 31, 45)).astype(np.float32)
+    out["half_in"] = half_in
+    out["half_out"] = np.stack([D._half(x) for x in half_in])
+    np.savez_compressed(os.path.join(HERE, "helpers.npz"), **out)
+
+
+def pm_case(R):
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c1", seed=5, width=40, height=32)
+    ref = sc.grey(sc.ref)
+    srcs = [sc.grey(s) for s in sc.srcs[:3]]
+    H, W = ref.shape
+    ray = O.rays_world((H, W), sc.ref_cam)
+    par = np.array([c.row() for c in sc.src_cams[:3]], np.float64)
+    rng = np.random.default_rng(9)
+    depth = (sc.depth_true * (1 + rng.normal(0, 0.01, (H, W)))).astype(np.float32)
+    depth[rng.random((H, W)) < 0.05] = np.nan
+    normal = S.tilted_normals(H, W, 11)        # +z: facing the nadir camera (rays point down)
+    score = np.zeros((H, W), np.float32)
+    active = (rng.random((H, W)) < 0.8).astype(np.uint8)
+    sdeps = [None, np.ascontiguousarray(sc.depth_true[:H, :W] * 1.001, np.float32), None]
+    args = dict(r=2, step=1, top_k=2, geo_w=0.5, geo_tol=0.02, iters=2, dmin=35.0, dmax=55.0, seed=12345)
+    out = {"ref": ref, "ray": ray, "par": par, "Cr": np.asarray(sc.ref_cam.C, np.float64), "depth0": depth.copy(),
+           "normal0": normal.copy(), "score0": score.copy(), "active": active, "sdep1": sdeps[1],
+           "args": np.array([args["r"], args["step"], args["top_k"], args["iters"], args["seed"]]),
+           "fargs": np.array([args["geo_w"], args["geo_tol"], args["dmin"], args["dmax"]])}
+    for j, s in enumerate(srcs):
+        out[f"src{j}"] = s
+    ch = R._dense.pm_refine(ref, ray, out["Cr"], srcs, sdeps, par, depth, normal, score, active, args["r"],
+                            args["step"], args["top_k"], args["geo_w"], args["geo_tol"], args["iters"], args["dmin"],
+                            args["dmax"], args["seed"])
+    out.update({"depth": depth, "normal": normal, "score": score, "changed": np.array(ch)})
+    np.savez_compressed(os.path.join(HERE, "pm_case.npz"), **out)
+
+
+def main():
+    D = refpkg.load_densify()
+    R = O.reference()
+    if D is None or R is None:
+        raise SystemExit("the reference is not available here: build oracle/_ref first (make -C oracle ref)")
+    sweep_cases(R)
+    sweep_e2e(D)
+    scene_small(D)
+    helpers(D, R)
+    pm_case(R)
+    for f in sorted(os.listdir(HERE)):
+        if f.endswith(".npz"):
+            print(f, os.path.getsize(os.path.join(HERE, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,114 @@
+"""The C ABI without a GPU: the library loads, exports every function include/mvs_b200.h
+declares, the ctypes structs match the C layout (gcc probe), and argument validation returns the
+reference's error classes before any device work."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "mvs_b200.h")
+
+
+def _lib():
+    from py_ortho_b200 import _lib as L
+    return L
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(mvs_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_function():
+    L = _lib()
+    lib = ctypes.CDLL(L.LIB_PATH)
+    names = declared_functions()
+    assert len(names) >= 18
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) == set(L.SIGNATURES), set(names) ^ set(L.SIGNATURES)
+    assert L.load().mvs_version().startswith(b"libmvs_b200")
+
+
+def test_ctypes_structs_match_the_c_layout(tmp_path):
+    L = _lib()
+    structs = {"mvs_hyp": L.Hyp, "mvs_sweep_args": L.SweepArgs, "mvs_pm_args": L.PMArgs,
+               "mvs_batch_job": L.BatchJob, "mvs_batch_tuning": L.BatchTuning}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("return 0; }")
+    c = tmp_path / "probe.c"
+    c.write_text("\n".join(lines))
+    exe = tmp_path / "probe"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(c)], check=True)
+    out = dict(l.rsplit(" ", 1) for l in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.split("\n") if l)
+    for cname, py in structs.items():
+        assert int(out[cname]) == ctypes.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert int(out[f"{cname}.{fname}"]) == getattr(py, fname).offset, (cname, fname)
+
+
+def test_validation_errors_need_no_device():
+    L = _lib()
+    lib = L.load()
+    a = L.SweepArgs()
+    a.n_src = 0
+    assert lib.mvs_sweep(ctypes.addressof(a), None) == L.ERR_VALUE
+    assert "1..16 sources" in L.last_error()
+    a.n_src = 17
+    assert lib.mvs_sweep(ctypes.addressof(a), None) == L.ERR_VALUE
+    a.n_src, a.r = 2, -1
+    assert lib.mvs_sweep(ctypes.addressof(a), None) == L.ERR_VALUE
+    assert "negative window radius" in L.last_error()
+    a.r = 9
+    geo = np.zeros((2, 18))
+    a.geo = geo.ctypes.data
+    a.top_k = 2
+    assert lib.mvs_sweep(ctypes.addressof(a), None) == L.ERR_UNSUPPORTED
+    with pytest.raises(NotImplementedError):
+        L.check(L.ERR_UNSUPPORTED)
+    with pytest.raises(ValueError):
+        L.check(L.ERR_VALUE)
+    with pytest.raises(MemoryError):
+        L.check(L.ERR_MEMORY)
+    with pytest.raises(TimeoutError):
+        L.check(L.ERR_TIMEOUT)
+    assert lib.mvs_box_zero_mean(4, 4, None, -1, 0, None, None) == L.ERR_VALUE
+    assert lib.mvs_box_zero_mean(0, 4, None, 1, 0, None, None) == L.OK        # empty input: no work
+    # PatchMatch with 0 or > 16 sources returns without work, as the reference does
+    p = L.PMArgs()
+    p.S = 0
+    assert lib.mvs_pm_refine(ctypes.addressof(p), None) == L.OK
+    p.S = 17
+    assert lib.mvs_pm_refine(ctypes.addressof(p), None) == L.OK
+    assert lib.mvs_batch_create(None, 0, None, ctypes.byref(ctypes.c_void_p())) == L.ERR_VALUE
+
+
+def test_python_layer_validates_before_touching_the_device():
+    from py_ortho_b200 import dense
+    with pytest.raises(ValueError, match="1..16 sources"):
+        dense.sweep_hypothesis(None, None, None, [], None, np.zeros((0, 18)), None, 1, 2, 0, None, None, None, None,
+                               None)
+    with pytest.raises(ValueError, match="geo must be"):
+        dense.sweep_hypothesis(None, None, None, [np.zeros((2, 2), np.float32)], None, np.zeros((2, 18)), None, 1, 2,
+                               0, None, None, None, None, None)
+    assert dense.pm_refine(None, None, None, [], [], None, None, None, None, None, 1, 1, 2, 0.0, 1.0, 1, 0, 1, 0) == 0
+
+
+def test_counter_draws_agree_with_the_oracle():
+    from oracle import oracle as O
+    lib = _lib().load()
+    for seed in (1, 99, 4294967295):
+        for pix in (0, 5, 10 ** 9):
+            for d in range(8):
+                assert lib.mvs_pm_uniform(seed, 2, pix, d) == O.pm_uniform(seed, 2, pix, d)

@@ -1,0 +1,76 @@
+"""Shared helpers of the test suite: seeded random sweep cases and the parity bar."""
+import numpy as np
+
+# The parity bar of the depth-map path (fixed by the project's specification):
+GAP = 1e-3          # winner index must match exactly where best - second best > GAP
+DEPTH_REL = 1e-3    # depth within 0.1 % relative where the winner index matches
+SCORE_ABS = 2e-4    # FP32 window sums vs the reference's float64 running sums
+FLIP_FRAC = 5e-3    # index flips are allowed only at near-ties, on at most 0.5 % of pixels
+
+
+def rotation(rng, tilt):
+    w = rng.normal(0, tilt, 3) + np.array([np.pi, 0, 0])
+    th = np.linalg.norm(w)
+    k = w / th
+    K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K
+
+
+def random_sweep_case(rng, H, W, n, nhyp, nan_frac=0.02):
+    """Random textured reference / sources with NaN masks, size jitter, distorted cameras and
+    per-pixel hypothesis maps (inv = inf and inv < 0 injected)."""
+    ref = rng.normal(0, 1, (H, W)).astype(np.float32)
+    srcs = []
+    for _ in range(n):
+        h = max(H + int(rng.integers(-3, 4)), 2)
+        w = max(W + int(rng.integers(-3, 4)), 2)
+        s = rng.normal(0, 1, (h, w)).astype(np.float32)
+        s[rng.random(s.shape) < nan_frac] = np.nan
+        srcs.append(np.ascontiguousarray(s))
+    ray = rng.normal(0, 0.3, (3, H, W)).astype(np.float32)
+    ray[2] = 1.0 + rng.normal(0, 0.01, (H, W)).astype(np.float32)
+    geo = []
+    for _ in range(n):
+        Rs = rotation(rng, 0.05) @ rotation(rng, 0.0).T
+        b = rng.normal(0, 0.5, 3)
+        f = float(rng.uniform(0.8, 1.2) * W)
+        geo.append(np.r_[Rs.ravel(), b, [f, rng.normal(0, 0.05), rng.normal(0, 0.01), rng.normal(0, 0.003),
+                                         (W - 1) / 2 + rng.normal(0, 2), (H - 1) / 2 + rng.normal(0, 2)]])
+    base = rng.uniform(0.02, 0.2, (H, W)).astype(np.float32)
+    step = rng.uniform(1e-4, 5e-3, (H, W)).astype(np.float32)
+    hyps = np.stack([(base + i * step).astype(np.float32) for i in range(nhyp)])
+    if nhyp > 2:
+        hyps[1, 0, 0] = np.inf
+        hyps[2, -1, -1] = -0.01
+    return ref, srcs, ray, np.array(geo, np.float64), hyps
+
+
+def gap_of(scores: np.ndarray) -> np.ndarray:
+    """best minus second-best hypothesis score per pixel from an (n, H, W) score volume."""
+    if scores.shape[0] < 2:
+        return np.full(scores.shape[1:], np.inf, np.float32)
+    s = np.sort(scores, axis=0)
+    return (s[-1] - s[-2]).astype(np.float32)
+
+
+def check_parity(idx, depth, best, ref_idx, ref_depth, ref_best, gap, label=""):
+    """The parity bar; returns a dict of the measured agreement for reporting."""
+    idx, ref_idx = np.asarray(idx), np.asarray(ref_idx)
+    decided = gap > GAP
+    bad = decided & (idx != ref_idx)
+    assert not bad.any(), f"{label}: winner index differs on {int(bad.sum())} decided pixels"
+    same = idx == ref_idx
+    flips = (~same).mean()
+    assert flips <= FLIP_FRAC, f"{label}: {flips:.4%} index flips at near-ties"
+    out = {"pixels": int(idx.size), "flips": int((~same).sum()), "decided": int(decided.sum())}
+    if depth is not None:
+        d, rd = np.asarray(depth, np.float64), np.asarray(ref_depth, np.float64)
+        fin = same & np.isfinite(rd) & (rd > 0)
+        rel = np.abs(d[fin] - rd[fin]) / rd[fin]
+        assert rel.size == 0 or rel.max() <= DEPTH_REL, f"{label}: depth rel error {rel.max():.3e}"
+        out["depth_rel_max"] = float(rel.max()) if rel.size else 0.0
+    if best is not None:
+        e = np.abs(np.asarray(best) - np.asarray(ref_best))[same]
+        assert e.size == 0 or e.max() <= SCORE_ABS, f"{label}: score error {e.max():.3e}"
+        out["score_abs_max"] = float(e.max()) if e.size else 0.0
+    return out
