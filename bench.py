@@ -206,15 +206,16 @@ def run_ours(a):
                 acc["pm"] += ev["pm"][0].elapsed_time(ev["pm"][1])
 
     setup_s = time.time() - t0
-    for _ in range(a.warmup):
-        step(False)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
     # device-time of the K timed steps (events around the whole loop), plus per-kernel events
-    # measured in a second pass so that their syncs do not enter the whole-step number
+    # measured in a second pass so that their syncs do not enter the whole-step number; the clock
+    # sampler starts before the warm-up so that its start-up never falls inside the timed region
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
+        for _ in range(a.warmup):
+            step(False)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         torch.cuda.synchronize()
         e0.record(stream)
         for _ in range(a.steps):

@@ -226,6 +226,26 @@ mvs_status mvs_batch_run(mvs_batch* b, int32_t use_graph, void* stream);
 mvs_status mvs_batch_stats(const mvs_batch* b, int64_t* work_items, int64_t* evals);
 void mvs_batch_destroy(mvs_batch* b);
 
+/* ---------------------------------------------------------------- continuous batching */
+
+/* A serving engine: a device table of `max_slots` resident jobs (MVS_HYP_PLANES sweeps) and a
+ * work-item buffer. Each step runs the next plane chunk of any set of resident jobs - all their
+ * tiles - in ONE persistent launch, then merges each chunk into that job's winner state in
+ * hypothesis order. Jobs join and leave between steps; a job's result does not depend on which
+ * other jobs share its steps. */
+typedef struct mvs_server mvs_server;
+
+mvs_status mvs_server_create(int32_t max_slots, int32_t max_items, int32_t max_radius, int32_t precision,
+                             mvs_server** out);
+/* Installs `job` in `slot`: its images, state arrays (initialised by the caller to the sweep's
+ * initial state) and hypotheses stay where the caller put them; `chunk_rec` is a device buffer
+ * of 6 * H * W floats for one chunk record; planes are processed `plane_chunk` at a time. */
+mvs_status mvs_server_set_job(mvs_server* s, int32_t slot, const mvs_sweep_args* job, float* chunk_rec,
+                              int32_t plane_chunk);
+/* Runs chunk chunks[k] of the job in slots[k], for k < n, in one launch and merges them. */
+mvs_status mvs_server_step(mvs_server* s, const int32_t* slots, const int32_t* chunks, int32_t n, void* stream);
+void mvs_server_destroy(mvs_server* s);
+
 /* ---------------------------------------------------------------- misc */
 
 /* Message of this thread's last failing call ("" if none). Returns the message length. */

@@ -81,6 +81,10 @@ SIGNATURES = {
     "mvs_batch_run": (i32, [vp, i32, vp]),
     "mvs_batch_stats": (i32, [vp, vp, vp]),
     "mvs_batch_destroy": (None, [vp]),
+    "mvs_server_create": (i32, [i32, i32, i32, i32, vp]),
+    "mvs_server_set_job": (i32, [vp, i32, vp, vp, i32]),
+    "mvs_server_step": (i32, [vp, vp, vp, i32, vp]),
+    "mvs_server_destroy": (None, [vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_version": (C.c_char_p, []),
 }

@@ -45,7 +45,9 @@ __global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restr
         const SweepParams& p = jobs[w.x];
         const int pa = p.i0 + w.w * p.ppc;
         const int pb = min(p.i1, pa + p.ppc);
-        sweep_tile<RMAX, true, KMAX, true, F16>(p, p.r, w.y * TW, w.z * TH, pa, pb, p.rec ? w.w : -1, smem);
+        // a job with one record buffer (nchunks == 1: serving) always writes record 0
+        sweep_tile<RMAX, true, KMAX, true, F16>(p, p.r, w.y * TW, w.z * TH, pa, pb,
+                                                p.rec ? (p.nchunks == 1 ? 0 : w.w) : -1, smem);
     }
 }
 
@@ -296,3 +298,181 @@ extern "C" mvs_status mvs_batch_stats(const mvs_batch* b, int64_t* work_items, i
 }
 
 extern "C" void mvs_batch_destroy(mvs_batch* b) { batch_free(b); }
+
+// ------------------------------------------------------------------------------ serving engine
+
+namespace mvs {
+
+struct StepMerge {                     // one (job, chunk) of a serving step
+    long long block0;
+    long long HW;
+    int pa, pb;
+    const float* rec;
+    float* best;
+    float* prev;
+    float* spb;
+    float* snb;
+    int* idx;
+};
+
+__global__ void server_merge_kernel(const StepMerge* __restrict__ m, int n) {
+    int lo = 0, hi = n - 1;
+    const long long blk = blockIdx.x;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (m[mid].block0 <= blk) lo = mid; else hi = mid - 1;
+    }
+    const StepMerge& j = m[lo];
+    const long long o = (blk - j.block0) * blockDim.x + threadIdx.x;
+    if (o >= j.HW) return;
+    float B = j.best[o], P = j.prev[o], SP = j.spb[o], SN = j.snb[o];
+    int I = j.idx[o];
+    merge_pixel(o, j.HW, 1, j.pa, j.pb, j.pb - j.pa, j.rec, B, P, SP, SN, I);
+    j.best[o] = B;
+    j.prev[o] = P;
+    j.spb[o] = SP;
+    j.snb[o] = SN;
+    j.idx[o] = I;
+}
+
+}  // namespace mvs
+
+struct mvs_server {
+    int max_slots = 0, max_items = 0, rmax = 3;
+    bool f16 = false;
+    int kmax = 2;
+    int grid = 0;
+    SweepParams* d_params = nullptr;
+    std::vector<SweepParams> h_params;
+    std::vector<char> used;
+    int4* d_items = nullptr;
+    int4* h_items = nullptr;           // pinned
+    StepMerge* d_merge = nullptr;
+    StepMerge* h_merge = nullptr;      // pinned
+    int* d_counter = nullptr;
+    cudaEvent_t uploaded = nullptr;
+};
+
+static void server_free(mvs_server* s) {
+    if (!s) return;
+    if (s->uploaded) cudaEventDestroy(s->uploaded);
+    cudaFree(s->d_params);
+    cudaFree(s->d_items);
+    cudaFree(s->d_merge);
+    cudaFree(s->d_counter);
+    cudaFreeHost(s->h_items);
+    cudaFreeHost(s->h_merge);
+    delete s;
+}
+
+extern "C" mvs_status mvs_server_create(int32_t max_slots, int32_t max_items, int32_t max_radius, int32_t precision,
+                                        mvs_server** out) {
+    clear_error();
+    if (!out) return fail(MVS_ERR_VALUE, "server: null output handle");
+    *out = nullptr;
+    if (max_slots < 1 || max_items < 1) return fail(MVS_ERR_VALUE, "server: needs slots and items");
+    if (max_radius < 0 || max_radius > MVS_MAX_RADIUS) return fail(MVS_ERR_VALUE, "server: radius outside 0..%d", MVS_MAX_RADIUS);
+    if (precision != MVS_PREC_FP32 && precision != MVS_PREC_FP16) return fail(MVS_ERR_VALUE, "server: unknown precision");
+    mvs_server* s = new mvs_server();
+    s->max_slots = max_slots;
+    s->max_items = max_items;
+    s->rmax = max_radius <= 3 ? 3 : 7;
+    s->f16 = precision == MVS_PREC_FP16;
+    s->h_params.resize(max_slots);
+    s->used.assign(max_slots, 0);
+    int cps = 0;
+    mvs_status st = s->rmax <= 3 ? (s->f16 ? batch_attr<3, 2, true>(&cps) : batch_attr<3, 2, false>(&cps))
+                                 : (s->f16 ? batch_attr<7, 2, true>(&cps) : batch_attr<7, 2, false>(&cps));
+    if (st != MVS_OK) { server_free(s); return st; }
+    s->grid = num_sms() * (cps > 0 ? cps : 1);
+    cudaError_t e = cudaMalloc((void**)&s->d_params, sizeof(SweepParams) * max_slots);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->d_items, sizeof(int4) * max_items);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->d_merge, sizeof(StepMerge) * max_slots);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->d_counter, sizeof(int));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_items, sizeof(int4) * max_items);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_merge, sizeof(StepMerge) * max_slots);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming);
+    if (e != cudaSuccess) { server_free(s); return fail(MVS_ERR_MEMORY, "server: allocation: %s", cudaGetErrorString(e)); }
+    *out = s;
+    return MVS_OK;
+}
+
+extern "C" mvs_status mvs_server_set_job(mvs_server* s, int32_t slot, const mvs_sweep_args* job, float* chunk_rec,
+                                         int32_t plane_chunk) {
+    clear_error();
+    if (!s || !job) return fail(MVS_ERR_VALUE, "server: null argument");
+    if (slot < 0 || slot >= s->max_slots) return fail(MVS_ERR_VALUE, "server: slot %d outside 0..%d", slot, s->max_slots - 1);
+    MVS_TRY(validate_sweep(job));
+    if (job->hyp.kind != MVS_HYP_PLANES) return fail(MVS_ERR_VALUE, "server: jobs must use MVS_HYP_PLANES");
+    if ((job->precision == MVS_PREC_FP16) != s->f16) return fail(MVS_ERR_VALUE, "server: job precision differs from the server's");
+    if (job->r > (s->rmax <= 3 ? 3 : 7)) return fail(MVS_ERR_VALUE, "server: job radius above the server's");
+    if (job->i1 - job->i0 > MVS_MAX_PLANES_PER_CALL || job->i1 <= job->i0) return fail(MVS_ERR_VALUE, "server: bad plane range");
+    if (job->H == 0 || job->W == 0) return fail(MVS_ERR_VALUE, "server: empty job");
+    if (!chunk_rec || plane_chunk < 1) return fail(MVS_ERR_VALUE, "server: needs a chunk record buffer and plane_chunk >= 1");
+    SweepParams p;
+    MVS_TRY(fill_params(job, p));
+    if (pick_kmax(p) > 2) return fail(MVS_ERR_UNSUPPORTED, "server: top_k needs more than 2 list entries");
+    const int n = job->i1 - job->i0;
+    for (int k = 0; k < n; ++k) p.planes[k] = job->hyp.planes[job->i0 + k];
+    p.i0 = job->i0;
+    p.i1 = job->i1;
+    p.r = job->r;
+    p.fresh = 1;
+    p.ppc = plane_chunk;
+    p.nchunks = 1;                     // one record buffer: chunk records always land in record 0
+    p.rec = chunk_rec;
+    s->h_params[slot] = p;
+    s->used[slot] = 1;
+    MVS_CUDA(cudaMemcpy(s->d_params + slot, &p, sizeof(SweepParams), cudaMemcpyHostToDevice), "server: upload job");
+    return MVS_OK;
+}
+
+extern "C" mvs_status mvs_server_step(mvs_server* s, const int32_t* slots, const int32_t* chunks, int32_t n,
+                                      void* stream) {
+    clear_error();
+    if (!s) return fail(MVS_ERR_VALUE, "server: null handle");
+    if (n <= 0) return MVS_OK;
+    if (!slots || !chunks || n > s->max_slots) return fail(MVS_ERR_VALUE, "server: bad step list");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    MVS_CUDA(cudaEventSynchronize(s->uploaded), "server: previous upload");   // host buffers free again
+    int items = 0;
+    long long blocks = 0;
+    for (int k = 0; k < n; ++k) {
+        const int sl = slots[k];
+        if (sl < 0 || sl >= s->max_slots || !s->used[sl]) return fail(MVS_ERR_VALUE, "server: slot %d holds no job", sl);
+        for (int q = 0; q < k; ++q)
+            if (slots[q] == sl) return fail(MVS_ERR_VALUE, "server: slot %d twice in one step", sl);
+        const SweepParams& p = s->h_params[sl];
+        const int pa = p.i0 + chunks[k] * p.ppc;
+        if (chunks[k] < 0 || pa >= p.i1) return fail(MVS_ERR_VALUE, "server: chunk %d beyond job %d", chunks[k], sl);
+        const int tx = (p.W + TW - 1) / TW, ty = (p.H + TH - 1) / TH;
+        if (items + tx * ty > s->max_items) return fail(MVS_ERR_VALUE, "server: step exceeds %d work items", s->max_items);
+        for (int y = 0; y < ty; ++y)
+            for (int x = 0; x < tx; ++x) s->h_items[items++] = make_int4(sl, x, y, chunks[k]);
+        StepMerge& m = s->h_merge[k];
+        m.block0 = blocks;
+        m.HW = (long long)p.H * p.W;
+        m.pa = pa;
+        m.pb = std::min(p.i1, pa + p.ppc);
+        m.rec = p.rec;
+        m.best = p.best; m.prev = p.prev; m.spb = p.spb; m.snb = p.snb; m.idx = p.idx;
+        blocks += (m.HW + 255) / 256;
+    }
+    MVS_CUDA(cudaMemcpyAsync(s->d_items, s->h_items, sizeof(int4) * items, cudaMemcpyHostToDevice, st), "server: items");
+    MVS_CUDA(cudaMemcpyAsync(s->d_merge, s->h_merge, sizeof(StepMerge) * n, cudaMemcpyHostToDevice, st), "server: merge table");
+    MVS_CUDA(cudaEventRecord(s->uploaded, st), "server: record upload");
+    MVS_CUDA(cudaMemsetAsync(s->d_counter, 0, sizeof(int), st), "server: counter");
+    const dim3 grid(s->grid);
+    if (s->rmax <= 3) {
+        if (s->f16) batch_launch<3, 2, true>(grid, st, s->d_params, s->d_items, items, s->d_counter);
+        else batch_launch<3, 2, false>(grid, st, s->d_params, s->d_items, items, s->d_counter);
+    } else {
+        if (s->f16) batch_launch<7, 2, true>(grid, st, s->d_params, s->d_items, items, s->d_counter);
+        else batch_launch<7, 2, false>(grid, st, s->d_params, s->d_items, items, s->d_counter);
+    }
+    MVS_TRY(check_launch("server persistent kernel"));
+    server_merge_kernel<<<(unsigned)blocks, 256, 0, st>>>(s->d_merge, n);
+    return check_launch("server merge kernel");
+}
+
+extern "C" void mvs_server_destroy(mvs_server* s) { server_free(s); }

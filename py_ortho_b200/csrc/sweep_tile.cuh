@@ -311,6 +311,8 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
                     jv[4 * q] = a.x; jv[4 * q + 1] = a.y; jv[4 * q + 2] = a.z; jv[4 * q + 3] = a.w;
                     iv[4 * q] = b.x; iv[4 * q + 1] = b.y; iv[4 * q + 2] = b.z; iv[4 * q + 3] = b.w;
                 }
+                // explicit rounding (no contraction) so that every instantiation - static or
+                // runtime radius - produces the same bits
                 float v[NIN], s1[NIN], s2[NIN], s3[NIN];
 #pragma unroll
                 for (int t = 0; t < NIN; ++t) {
@@ -318,15 +320,18 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
                     const float jz = ok ? jv[t] : 0.f;
                     v[t] = ok ? 1.f : 0.f;
                     s1[t] = jz;
-                    s2[t] = jz * jz;
-                    s3[t] = jz * iv[t];
+                    s2[t] = __fmul_rn(jz, jz);
+                    s3[t] = __fmul_rn(jz, iv[t]);
                 }
                 float o0[4], o1[4], o2[4], o3[4];
                 float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
                 for (int t = -RMAX; t <= RMAX; ++t) {
                     if (t >= -r && t <= r) {
-                        a0 += v[RA + t]; a1 += s1[RA + t]; a2 += s2[RA + t]; a3 += s3[RA + t];
+                        a0 = __fadd_rn(a0, v[RA + t]);
+                        a1 = __fadd_rn(a1, s1[RA + t]);
+                        a2 = __fadd_rn(a2, s2[RA + t]);
+                        a3 = __fadd_rn(a3, s3[RA + t]);
                     }
                 }
                 o0[0] = a0; o1[0] = a1; o2[0] = a2; o3[0] = a3;
@@ -348,10 +353,10 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
                         n0 = v[tn]; n1 = s1[tn]; n2 = s2[tn]; n3 = s3[tn];
                         d0 = v[to]; d1 = s1[to]; d2 = s2[to]; d3 = s3[to];
                     }
-                    a0 += n0 - d0;
-                    a1 += n1 - d1;
-                    a2 += n2 - d2;
-                    a3 += n3 - d3;
+                    a0 = __fadd_rn(a0, __fsub_rn(n0, d0));
+                    a1 = __fadd_rn(a1, __fsub_rn(n1, d1));
+                    a2 = __fadd_rn(a2, __fsub_rn(n2, d2));
+                    a3 = __fadd_rn(a3, __fsub_rn(n3, d3));
                     o0[j] = a0; o1[j] = a1; o2[j] = a2; o3[j] = a3;
                 }
                 float4* hp = reinterpret_cast<float4*>(sH + hy * TW + 4 * gi);
@@ -373,30 +378,33 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
                 for (int t = 0; t <= 2 * RMAX; ++t) {
                     if (t <= 2 * r) {
                         const int o = (y0 + t) * TW;
-                        cv += h0[o]; cj += h1[o]; cjj += h2[o]; cji += h3[o];
+                        cv = __fadd_rn(cv, h0[o]);
+                        cj = __fadd_rn(cj, h1[o]);
+                        cjj = __fadd_rn(cjj, h2[o]);
+                        cji = __fadd_rn(cji, h3[o]);
                     }
                 }
 #pragma unroll
                 for (int j = 0; j < ROWS; ++j) {
                     if (j > 0) {
                         const int on = (y0 + j + 2 * r) * TW, oo = (y0 + j - 1) * TW;
-                        cv += h0[on] - h0[oo];
-                        cj += h1[on] - h1[oo];
-                        cjj += h2[on] - h2[oo];
-                        cji += h3[on] - h3[oo];
+                        cv = __fadd_rn(cv, __fsub_rn(h0[on], h0[oo]));
+                        cj = __fadd_rn(cj, __fsub_rn(h1[on], h1[oo]));
+                        cjj = __fadd_rn(cjj, __fsub_rn(h2[on], h2[oo]));
+                        cji = __fadd_rn(cji, __fsub_rn(h3[on], h3[oo]));
                     }
                     float ncc;
                     if (cv * 10.f <= 9.f * k2) {
                         ncc = -1.f;
                     } else {
                         const float rc = (cv == k2) ? inv_k2 : __frcp_rn(cv);
-                        const float mj = cj * rc, m2 = cjj * rc, mij = cji * rc;
-                        const float var = m2 - mj * mj;
+                        const float mj = __fmul_rn(cj, rc), m2 = __fmul_rn(cjj, rc), mij = __fmul_rn(cji, rc);
+                        const float var = __fsub_rn(m2, __fmul_rn(mj, mj));
                         const float rsdj = var > 1e-6f ? rsqrtf(var) : 1000.f;
-                        ncc = (mij - mu[j] * mj) * (rsd[j] * rsdj);
+                        ncc = __fmul_rn(__fsub_rn(mij, __fmul_rn(mu[j], mj)), __fmul_rn(rsd[j], rsdj));
                         ncc = ncc > 1.f ? 1.f : (ncc < -1.f ? -1.f : ncc);
                     }
-                    total[j] += ncc;
+                    total[j] = __fadd_rn(total[j], ncc);
                     float x = ncc;
 #pragma unroll
                     for (int q = 0; q < KMAX; ++q) {
@@ -415,8 +423,8 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
             float s = 0.f;
 #pragma unroll
             for (int q = 0; q < KMAX; ++q)
-                if (q < nlist) s = s + topk[j][q];
-            if (bottom) s = total[j] - s;
+                if (q < nlist) s = __fadd_rn(s, topk[j][q]);
+            if (bottom) s = __fsub_rn(total[j], s);
             s = __fdiv_rn(s, (float)kk);
             if (idx[j] == i - 1) snb[j] = s;
             if (s > best[j]) {

@@ -6,9 +6,9 @@ benchmark configurations):
   buildings (3-12 m above the terrain at their centre);
 * texture: 4-octave value noise (periods 3, 6, 12, 24 ground pixels) of (x + 0.37 z, y - 0.61 z),
   quantised to uint8 grey (walls get texture that varies with height);
-* nadir pinhole cameras (R = diag(1, -1, -1), image x = east, y = south, principal point at the
-  image centre, pixel centres at integers), rendered by ray casting the heightfield: a 0.25 m
-  march along camera-axis depth, then 24 bisection steps.
+* nadir pinhole cameras (R = diag(1, -1, -1) with a seeded 0.3 deg attitude error, image x = east,
+  y = south, principal point at the image centre, pixel centres at integers), rendered by ray
+  casting the heightfield: a 0.25 m march along camera-axis depth, then 24 bisection steps.
 
 Rendering uses torch and runs on any device (CPU for the small test scenes, the GPU for the
 full-size ones); it is set-up work, outside every timed region.
@@ -43,6 +43,21 @@ class Camera:
 
 
 NADIR = np.diag([1.0, -1.0, -1.0])
+
+
+def attitude(rng, sigma_deg: float) -> np.ndarray:
+    """World -> camera rotation of a nadir camera with a small seeded attitude error (Rodrigues
+    rotation of normal(0, sigma) radians per axis applied after the nadir rotation). Real
+    flights never have exactly parallel optical axes; without it the along-track sources would
+    map image edges exactly onto source image edges, a measure-zero tie of the sample-validity
+    test that rounding decides arbitrarily."""
+    w = rng.normal(0.0, np.radians(sigma_deg), 3)
+    th = float(np.linalg.norm(w))
+    if th == 0.0:
+        return NADIR.copy()
+    k = w / th
+    K = np.array([[0, -k[2], k[1]], [k[2], 0, -k[0]], [-k[1], k[0], 0]])
+    return (np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * K @ K) @ NADIR
 
 
 @dataclass
@@ -256,8 +271,10 @@ def make_scene(cfg: SceneConfig | str, seed: int = 0, device="cpu", width: int |
     terr = _terrain(cfg, seed, half_x, half_y)
     terr.gsd = cfg.altitude / f
 
+    att = np.random.default_rng(seed + 7777)
+
     def cam_at(x, y):
-        return Camera(NADIR.copy(), np.array([x, y, cfg.altitude]), f, (W - 1) / 2.0, (H - 1) / 2.0, W, H)
+        return Camera(attitude(att, 0.3), np.array([x, y, cfg.altitude]), f, (W - 1) / 2.0, (H - 1) / 2.0, W, H)
 
     ref_cam = cam_at(0.0, 0.0)
     src_cams = [cam_at(x, y) for x, y in source_offsets(cfg)]

@@ -154,11 +154,16 @@ def test_densify_sweep_dropin_end_to_end():
     assert same_bits(sd, z["sd"])                       # window statistics are bit-exact
     full = O.sweep(z["ref"], srcs, z["ray"], z["geo"], list(z["hyps"]), r, top_k, keep_scores=True)
     assert same_bits(full["depth"], z["depth"])
+    # this geometry (the reference's own end-to-end test shape) leaves every window below the
+    # 90 % validity threshold: all scores tie at -1, the first hypothesis wins and the depth is
+    # its own - which must be reproduced exactly
+    ties = np.all(full["scores"] == -1.0, axis=0)
+    assert same_bits(best[ties], z["best"][ties]) and same_bits(depth[ties], z["depth"][ties])
     decided = gap_of(full["scores"]) > 1e-3            # _sweep returns no index: use the gap mask
     rel = np.abs(depth.astype(np.float64) - z["depth"]) / np.abs(z["depth"])
     ok = decided & np.isfinite(rel)
-    assert rel[ok].max() <= 1e-3
-    assert np.abs(best - z["best"])[decided].max() <= SCORE_ABS
+    assert not ok.any() or rel[ok].max() <= 1e-3
+    assert not decided.any() or np.abs(best - z["best"])[decided].max() <= SCORE_ABS
 
 
 def test_finalize_is_bit_exact_given_the_state():
