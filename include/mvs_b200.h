@@ -108,6 +108,19 @@ typedef struct mvs_sweep_args {
  * Needs device scratch when plane_chunks > 1 (allocated stream-ordered per call). */
 mvs_status mvs_sweep(const mvs_sweep_args* args, void* stream);
 
+/* mvs_sweep for callers that cannot allocate device memory - a process whose device memory is
+ * owned by another allocator with a fixed budget, or a latency-critical loop that must not enter
+ * the driver's allocator (cudaMalloc can synchronise the device). No counterpart in the
+ * reference (its CPU kernel mallocs per call). Same arguments and results as mvs_sweep, but the
+ * plane-chunk scratch is one 32 MiB file-scope device array per GPU, held until the process
+ * exits: with plane_chunks = 0 the chunk count is lowered until the records fit; an explicit
+ * plane_chunks whose records (6 floats per pixel per chunk) exceed 32 MiB gives MVS_ERR_VALUE.
+ * The first call on a device looks the array up (with that device current): make it before
+ * any stream capture. All calls share the array and it keeps the last call's contents (none of
+ * it needs to start at zero); calls that overlap on the GPU race on it. Calls no cudaMalloc,
+ * cudaFree or other allocating routine. */
+mvs_status mvs_sweep_noalloc(const mvs_sweep_args* args, void* stream);
+
 /* One hypothesis `i` given as an explicit inverse-depth map `inv` (H, W), ray-grid geometry
  * with radial distortion. Replaces _dense.sweep_hypothesis (_dense.pyx:740-838); argument
  * order and meaning as there (srcs: n_src device pointers with their shapes). */

@@ -64,6 +64,7 @@ class BatchTuning(C.Structure):
 # name -> (restype, argtypes); every symbol the header declares
 SIGNATURES = {
     "mvs_sweep": (i32, [vp, vp]),
+    "mvs_sweep_noalloc": (i32, [vp, vp]),
     "mvs_sweep_hypothesis": (i32, [i32, i32, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp, i32, i32, i32,
                                    vp, vp, vp, vp, vp, vp]),
     "mvs_sweep_finalize": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp]),

@@ -24,7 +24,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 EXTRA = {
     "patchmatch.cu": ["-fmad=false"],
 }
-SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu"]
+SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu", "noalloc.cu"]
 
 
 def nvcc() -> str:
