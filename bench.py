@@ -46,6 +46,12 @@ def parse():
     ap.add_argument("--pm-iters", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--mode", choices=["headline", "batch", "serve"], default="headline",
+                    help="headline: the single-view step above; batch: 64 uneven views in one persistent "
+                         "launch vs per-view launches; serve: Poisson arrivals through the continuous-batching server")
+    ap.add_argument("--jobs", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (jobs/s)")
+    ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
 
@@ -486,10 +492,200 @@ def run_reference(a):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------------------ batched / served views
+class _CropCam:
+    """A crop of a pinhole camera: same pose and focal length, shifted principal point."""
+
+    def __init__(self, cam, x0, y0, w, h):
+        self.R, self.C, self.f = cam.R, cam.C, cam.f
+        self.k1 = self.k2 = self.k3 = 0.0
+        self.cx, self.cy, self.w, self.h = cam.cx - x0, cam.cy - y0, w, h
+
+
+def flight(dev, seed=0, grid=4, W=4000, H=3000):
+    """A seeded grid flight (75 % overlap both ways) of nadir views over one terrain, rendered at
+    W x H on the device: the image pool of the batched / served configurations."""
+    from py_ortho_b200 import scene as S
+    cfg = S.CONFIGS["c2"]
+    import dataclasses
+    cfg = dataclasses.replace(cfg, forward_overlap=0.75, side_overlap=0.75)
+    fx = W * cfg.altitude / cfg.focal * 0.25
+    fy = H * cfg.altitude / cfg.focal * 0.25
+    span_x, span_y = fx * (grid - 1), fy * (grid - 1)
+    terr = S._terrain(cfg, seed, 0.5 * span_x + 0.5 * W * cfg.altitude / cfg.focal + 25.0,
+                      0.5 * span_y + 0.5 * H * cfg.altitude / cfg.focal + 25.0)
+    terr.gsd = cfg.altitude / cfg.focal
+    att = np.random.default_rng(seed + 7777)
+    cams, imgs = [], []
+    for gy in range(grid):
+        for gx in range(grid):
+            cam = S.Camera(S.attitude(att, 0.3), np.array([gx * fx - 0.5 * span_x, gy * fy - 0.5 * span_y, cfg.altitude]),
+                           cfg.focal, (W - 1) / 2.0, (H - 1) / 2.0, W, H)
+            img, _ = S.render(cam, terr, dev)
+            cams.append(cam)
+            imgs.append(img)
+    return cfg, cams, imgs
+
+
+def view_jobs(n_jobs, cams, imgs, dev, seed, prec=None):
+    """Config-4 jobs: reference = a random 4:3 crop (long side U(1200, 4000)) of one of the central
+    views, sources = its 4..12 nearest other views (device-resident, shared), planes U{96..384}
+    over [60, 90] m, window 5x5 or 7x7."""
+    import torch
+    from py_ortho_b200 import scene as S
+    rng = np.random.default_rng(seed)
+    grey = [torch.from_numpy(((im.astype(np.float32) - 128.0) / 64.0).astype(np.float32)).to(dev) for im in imgs]
+    n = len(cams)
+    g = int(round(n ** 0.5))
+    central = [y * g + x for y in range(1, g - 1) for x in range(1, g - 1)] or [0]
+    jobs = []
+    for k in range(n_jobs):
+        rv = central[k % len(central)]
+        L_ = int(rng.integers(1200, 4001))
+        w, h = L_, (3 * L_) // 4
+        x0 = int(rng.integers(0, 4000 - w + 1))
+        y0 = int(rng.integers(0, 3000 - h + 1))
+        ns = int(rng.integers(4, 13))
+        others = sorted((j for j in range(n) if j != rv),
+                        key=lambda j: np.linalg.norm(np.asarray(cams[j].C) - np.asarray(cams[rv].C)))[:ns]
+        planes = S.plane_list(60.0, 90.0, int(rng.integers(96, 385)))
+        r = int(rng.choice([2, 3]))
+        jobs.append(dict(ref=grey[rv][y0:y0 + h, x0:x0 + w].contiguous(), ref_cam=_CropCam(cams[rv], x0, y0, w, h),
+                         srcs=[grey[j] for j in others], src_cams=[cams[j] for j in others], planes=planes, r=r,
+                         ref_u8=imgs[rv][y0:y0 + h, x0:x0 + w]))
+    return jobs
+
+
+def run_batch(a):
+    """Config 4: per-view launches (plain single-view kernel) vs one persistent batched launch in
+    a CUDA graph (autotuned plane chunk / CTAs per SM), FP32 and FP16 storage."""
+    import torch
+    from py_ortho_b200 import _lib as L, batch, dense, fast
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    cfg, cams, imgs = flight(dev, a.seed)
+    jobs = view_jobs(a.jobs, cams, imgs, dev, a.seed)
+    setup = time.time() - t0
+    evals = sum(int(j["ref"].numel()) * len(j["planes"]) * len(j["srcs"]) for j in jobs)
+    st = torch.cuda.current_stream()
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    vj = [batch.ViewJob(j["ref"], j["srcs"], j["ref_cam"], j["src_cams"], j["planes"], r=j["r"], top_k=2).prepare()
+          for j in jobs]
+    torch.cuda.synchronize()
+
+    def plain():
+        for v in vj:
+            hyp = dense.Hypotheses.planes_inv(v.planes_inv)
+            stt = dense.sweep(v.ref, v.mu, v.sd, None, v.srcs, batch._geo(v.ref_cam, v.src_cams), hyp, v.r, v.top_k,
+                              state=v.state, ref_cam=fast.cam_row(v.ref_cam))
+            dense.finalize(hyp, stt, out=v.depth)
+            for t in v.state[:4]:
+                t.fill_(-2.0)
+            v.state[4].fill_(-1)
+
+    ms_plain = timed(plain)
+    d_plain = [v.depth.clone() for v in vj]
+    best, table = batch.autotune(vj, chunks=(0, 128), ctas=(0, 1), reps=1)
+    ms_batch = timed(lambda: best.run(graph=True), reps=2)
+    same = all(torch.equal(v.depth, d) for v, d in zip(vj, d_plain))
+    best.close()
+    # FP16 storage of the (shared) sources
+    h16 = {}
+    vj16 = []
+    for v in vj:
+        srcs16 = []
+        for s_ in v.srcs:
+            key = s_.data_ptr()
+            if key not in h16:
+                h16[key] = fast.to_fp16(s_)
+            srcs16.append(h16[key])
+        vj16.append(batch.ViewJob(v.ref, srcs16, v.ref_cam, v.src_cams, v.planes_inv, r=v.r, top_k=2).prepare())
+    best16, table16 = batch.autotune(vj16, precision=L.PREC_FP16, chunks=(0, 128), ctas=(0, 1), reps=1)
+    ms_16 = timed(lambda: best16.run(graph=True), reps=2)
+    rel = []
+    for v16, d in zip(vj16, d_plain):
+        x, y = v16.depth.double(), d.double()
+        m = torch.isfinite(x) & torch.isfinite(y) & (y > 0)
+        rel.append(((x - y).abs() / y)[m].cpu().numpy())
+    rel = np.concatenate(rel)
+    best16.close()
+    line = {"mode": "batch", "metric": "ZNCC evaluations/s (pixel x plane x view)", "unit": "Gpix.plane.view/s",
+            "jobs": len(jobs), "evals": evals, "setup_s": round(setup, 1),
+            "plain_per_view": {"ms": round(ms_plain, 2), "value": evals / (ms_plain / 1e3) / 1e9},
+            "batched_fp32": {"ms": round(ms_batch, 2), "value": evals / (ms_batch / 1e3) / 1e9,
+                             "identical_to_plain": bool(same), "autotune_ms": [(c, k, round(t, 2)) for c, k, t in table],
+                             "work_items": None},
+            "batched_fp16": {"ms": round(ms_16, 2), "value": evals / (ms_16 / 1e3) / 1e9,
+                             "depth_rel_err_vs_fp32_median": float(np.median(rel)),
+                             "depth_rel_err_vs_fp32_p99": float(np.percentile(rel, 99)),
+                             "autotune_ms": [(c, k, round(t, 2)) for c, k, t in table16]},
+            "speedup_fp16_batched_vs_plain": ms_plain / ms_16, "speedup_fp32_batched_vs_plain": ms_plain / ms_batch,
+            "config": {"workload": "c4: 64 views, long side U(1200,4000) 4:3, 4-12 sources, 96-384 planes, 5x5/7x7",
+                       "flight": "4x4 grid, 75 % overlap, 4000x3000, f=3600, 80 m; references are crops"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_serve(a):
+    """Config 5: Poisson arrivals through the continuous-batching server vs the plain
+    per-request path on the same trace; p50 / p99 latency and throughput."""
+    import torch
+    from py_ortho_b200 import serve as SV
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t0 = time.time()
+    cfg, cams, imgs = flight(dev, a.seed)
+    jobs = view_jobs(a.jobs, cams, imgs, dev, a.seed + 1)
+    rng = np.random.default_rng(a.seed + 2)
+    arrivals = np.cumsum(rng.exponential(1.0 / a.rate, len(jobs)))
+    pm = rng.random(len(jobs)) < 0.1
+
+    def trace():
+        out = []
+        for k, j in enumerate(jobs):
+            out.append(SV.DepthRequest(j["ref"].cpu().numpy(), j["srcs"], j["ref_cam"], j["src_cams"], j["planes"],
+                                       r=j["r"], top_k=2, pm_iters=4 if pm[k] else 0, pm_radius=3, pm_step=1,
+                                       depth_range=(60.0, 90.0), seed=k, arrival=float(arrivals[k]), rid=k))
+        return out
+
+    setup = time.time() - t0
+    evals = sum(q.evals for q in trace())
+    srv = SV.DepthServer(hbm_budget=120e9, max_slots=64, plane_chunk=32, shared_sources=True)
+    res_s, wall_s = SV.serve(trace(), srv, realtime=True)
+    srv.close()
+    res_p, wall_p = SV.serve_plain(trace(), realtime=True)
+    same = all(np.array_equal(x.depth, y.depth, equal_nan=True) for x, y in zip(res_s, res_p))
+    span_s = max(r.finished for r in res_s) - float(arrivals[0])
+    span_p = max(r.finished for r in res_p) - float(arrivals[0])
+    line = {"mode": "serve", "metric": "latency p50/p99 ms and ZNCC evaluations/s", "jobs": len(jobs),
+            "pm_jobs": int(pm.sum()), "rate_jobs_per_s": a.rate, "evals": evals, "setup_s": round(setup, 1),
+            "server": dict(SV.latency_stats(res_s), throughput=evals / span_s / 1e9, steps=srv.steps),
+            "plain": dict(SV.latency_stats(res_p), throughput=evals / span_p / 1e9),
+            "identical_results": bool(same), "unit_throughput": "Gpix.plane.view/s",
+            "config": {"workload": "c5: Poisson arrivals, c4 size/source/plane distribution, 10 % PatchMatch (4 it)",
+                       "hbm_budget_gb": 120, "plane_chunk": 32, "max_slots": 64}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
+    elif a.mode == "batch":
+        run_batch(a)
+    elif a.mode == "serve":
+        run_serve(a)
     else:
         run_ours(a)
 

@@ -46,8 +46,24 @@ __global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restr
         const int pa = p.i0 + w.w * p.ppc;
         const int pb = min(p.i1, pa + p.ppc);
         // a job with one record buffer (nchunks == 1: serving) always writes record 0
-        sweep_tile<RMAX, true, KMAX, true, F16>(p, p.r, w.y * TW, w.z * TH, pa, pb,
-                                                p.rec ? (p.nchunks == 1 ? 0 : w.w) : -1, smem);
+        const int ch = p.rec ? (p.nchunks == 1 ? 0 : w.w) : -1;
+        const int tx = w.y * TW, ty = w.z * TH;
+        // the radius is uniform per work item: each case is the single-view instance itself
+        switch (p.r) {
+            case 0: sweep_tile<0, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+            case 1: sweep_tile<1, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+            case 2: sweep_tile<2, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+            case 3: sweep_tile<3, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+            default:
+                if constexpr (RMAX > 3) {
+                    switch (p.r) {
+                        case 4: sweep_tile<4, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 5: sweep_tile<5, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 6: sweep_tile<6, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+                        default: sweep_tile<7, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+                    }
+                }
+        }
     }
 }
 
@@ -81,7 +97,7 @@ __global__ void batch_finalize_kernel(const JobFin* __restrict__ jobs, int n_job
 template <int RMAX, int KMAX, bool F16>
 static mvs_status batch_attr(int* max_ctas_per_sm) {
     auto kern = batch_kernel<RMAX, KMAX, F16>;
-    const size_t smem = Geom<RMAX>::smem_bytes();
+    const size_t smem = smem_bytes_upto<RMAX>();
     MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "batch: smem attribute");
     MVS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_ctas_per_sm, kern, NT, smem), "batch: occupancy");
     return MVS_OK;
@@ -89,7 +105,7 @@ static mvs_status batch_attr(int* max_ctas_per_sm) {
 
 template <int RMAX, int KMAX, bool F16>
 static void batch_launch(dim3 grid, cudaStream_t st, const SweepParams* jobs, const int4* items, int n, int* counter) {
-    batch_kernel<RMAX, KMAX, F16><<<grid, NT, Geom<RMAX>::smem_bytes(), st>>>(jobs, items, n, counter);
+    batch_kernel<RMAX, KMAX, F16><<<grid, NT, smem_bytes_upto<RMAX>(), st>>>(jobs, items, n, counter);
 }
 
 }  // namespace mvs
@@ -272,10 +288,11 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
 extern "C" mvs_status mvs_batch_run(mvs_batch* b, int32_t use_graph, void* stream) {
     clear_error();
     if (!b) return fail(MVS_ERR_VALUE, "batch: null handle");
-    cudaStream_t st = stream ? reinterpret_cast<cudaStream_t>(stream) : b->own_stream;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);   // NULL = legacy default stream
     if (!use_graph) return batch_enqueue(b, st);
     if (!b->exec) {
-        // capture on the private stream (capture is not possible on the legacy default stream)
+        // capture on the private stream (capture is not possible on the legacy default stream);
+        // the instantiated graph then runs on the caller's stream
         MVS_CUDA(cudaStreamBeginCapture(b->own_stream, cudaStreamCaptureModeThreadLocal), "batch: begin capture");
         mvs_status s = batch_enqueue(b, b->own_stream);
         cudaGraph_t g = nullptr;

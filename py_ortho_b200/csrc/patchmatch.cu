@@ -26,9 +26,12 @@ struct PMParams {
     float* score;
     const unsigned char* active;
     unsigned long long* changed;
+    double* cost_cache;                // per pixel; NaN = recompute (valid within one call)
+    double* score_cache;
     const float* img[MVS_MAX_SOURCES];
     const float* dep[MVS_MAX_SOURCES];
     int iw[MVS_MAX_SOURCES], ih[MVS_MAX_SOURCES];
+    int pinhole[MVS_MAX_SOURCES];       // k1 = k2 = k3 = 0
     double par[MVS_MAX_SOURCES * 18];
 };
 
@@ -78,8 +81,16 @@ __device__ __forceinline__ double pm_bil(const float* im, int w, int h, double u
     return (a00 * (1.0 - fx) + a01 * fx) * (1.0 - fy) + (a10 * (1.0 - fx) + a11 * fx) * fy;
 }
 
-// _pm_cost (_dense.pyx:461-556). Sources are the outer loop (per-source sums are independent,
-// so this changes no result) to keep five running sums in registers instead of 5 x 16.
+// _pm_cost (_dense.pyx:461-556). Window samples are the outer loop as in the reference; the
+// sources of a pass (PM_SRC_PASS at a time) are unrolled inside it with their five sums in
+// registers, so each sample's world point (one division) is formed once per pass instead of once
+// per source. Each source's work is branch-free (invalid samples read a safe address and add 0.0,
+// which leaves a sum that started at +0.0 unchanged), so the sources' float64 dependency chains
+// interleave. Every per-source sum still accumulates in window order: no result changes.
+#ifndef PM_SRC_PASS
+#define PM_SRC_PASS 2
+#endif
+
 __device__ double pm_cost(const PMParams& c, int y, int x, double d, const double* n, double& ncc_out) {
     const int H = c.H, W = c.W;
     const long long HW = (long long)H * W, idx = (long long)y * W + x;
@@ -92,12 +103,15 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
     const double num = d * ndr;
     double ncc[MVS_MAX_SOURCES];
     int nsamp = 0;
-    for (int s = 0; s < c.S; ++s) {
-        const double* par = c.par + 18 * s;
-        const float* im = c.img[s];
-        const int iw = c.iw[s], ih = c.ih[s];
-        double sI = 0.0, sJ = 0.0, sII = 0.0, sJJ = 0.0, sIJ = 0.0;
-        int cnt = 0, ns = 0;
+    for (int s0 = 0; s0 < c.S; s0 += PM_SRC_PASS) {
+        double sI[PM_SRC_PASS], sJ[PM_SRC_PASS], sII[PM_SRC_PASS], sJJ[PM_SRC_PASS], sIJ[PM_SRC_PASS];
+        int cnt[PM_SRC_PASS];
+#pragma unroll
+        for (int k = 0; k < PM_SRC_PASS; ++k) {
+            sI[k] = 0.0; sJ[k] = 0.0; sII[k] = 0.0; sJJ[k] = 0.0; sIJ[k] = 0.0; cnt[k] = 0;
+        }
+        const int npass = min(PM_SRC_PASS, c.S - s0);
+        int ns = 0;
         for (int a = -c.r; a <= c.r; a += c.step) {
             const int yy = y + a;
             if (yy < 0 || yy >= H) continue;
@@ -113,30 +127,64 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
                 const double t = num / den;
                 const double X = c.cr0 + t * qx, Y = c.cr1 + t * qy, Z = c.cr2 + t * qz;
                 ++ns;
-                double u, v, z;
-                if (pm_proj(par, X, Y, Z, u, v, z)) {
-                    const double J = pm_bil(im, iw, ih, u, v);
-                    if (isfinite(J)) {
-                        sI += I;
-                        sJ += J;
-                        sII += I * I;
-                        sJJ += J * J;
-                        sIJ += I * J;
-                        cnt += 1;
+                const double II = I * I;
+#pragma unroll
+                for (int k = 0; k < PM_SRC_PASS; ++k) {
+                    if (k < npass) {
+                        const int s = s0 + k;
+                        const double* p = c.par + 18 * s;
+                        // _proj
+                        const double dx = X - p[9], dy = Y - p[10], dz = Z - p[11];
+                        const double xc = p[0] * dx + p[1] * dy + p[2] * dz;
+                        const double yc = p[3] * dx + p[4] * dy + p[5] * dz;
+                        const double zc = p[6] * dx + p[7] * dy + p[8] * dz;
+                        const bool front = zc > 1e-6;
+                        const double zq = front ? zc : 1.0;
+                        const double nx = xc / zq, ny = yc / zq;
+                        // pinhole source: the reference's factor f (1 + r2 (k1 + r2 (k2 + r2 k3)))
+                        // evaluates to exactly f (r2 >= 0 finite, so every product with 0 is +0)
+                        double dd = p[12];
+                        if (!c.pinhole[s]) {
+                            const double r2 = nx * nx + ny * ny;
+                            dd = p[12] * (1.0 + r2 * (p[13] + r2 * (p[14] + r2 * p[15])));
+                        }
+                        const double u = dd * nx + p[16], v = dd * ny + p[17];
+                        // _bil with its bounds (NaN u / v count as outside)
+                        const int iw = c.iw[s], ih = c.ih[s];
+                        const bool in = front && u >= 0.0 && v >= 0.0 && u <= (double)iw - 1.001 && v <= (double)ih - 1.001;
+                        const double us = in ? u : 0.0, vs = in ? v : 0.0;
+                        const int x0 = (int)us, y0 = (int)vs;
+                        const double fx = us - (double)x0, fy = vs - (double)y0;
+                        const float* im = c.img[s] + ((long long)y0 * iw + x0);
+                        const double a00 = __ldg(im), a01 = __ldg(im + 1), a10 = __ldg(im + iw), a11 = __ldg(im + iw + 1);
+                        const double J = (a00 * (1.0 - fx) + a01 * fx) * (1.0 - fy) + (a10 * (1.0 - fx) + a11 * fx) * fy;
+                        const bool ok = in && isfinite(J);
+                        sI[k] += ok ? I : 0.0;
+                        sJ[k] += ok ? J : 0.0;
+                        sII[k] += ok ? II : 0.0;
+                        sJJ[k] += ok ? J * J : 0.0;
+                        sIJ[k] += ok ? I * J : 0.0;
+                        cnt[k] += ok ? 1 : 0;
                     }
                 }
             }
         }
-        nsamp = ns;   // identical for every source
-        if (ns < 4 || (double)cnt < 0.7 * (double)ns) {
-            ncc[s] = -1.0;
-        } else {
-            const double dc = (double)cnt;
-            const double mi = sI / dc, mj = sJ / dc;
-            const double vi = sII / dc - mi * mi;
-            const double vj = sJJ / dc - mj * mj;
-            const double cv = sIJ / dc - mi * mj;
-            ncc[s] = (vi < 1e-8 || vj < 1e-8) ? 0.0 : cv / sqrt(vi * vj);
+        nsamp = ns;   // identical for every pass
+#pragma unroll
+        for (int k = 0; k < PM_SRC_PASS; ++k) {
+            const int s = s0 + k;
+            if (k < npass) {
+                if (ns < 4 || (double)cnt[k] < 0.7 * (double)ns) {
+                    ncc[s] = -1.0;
+                } else {
+                    const double dc = (double)cnt[k];
+                    const double mi = sI[k] / dc, mj = sJ[k] / dc;
+                    const double vi = sII[k] / dc - mi * mi;
+                    const double vj = sJJ[k] / dc - mj * mj;
+                    const double cv = sIJ[k] / dc - mi * mj;
+                    ncc[s] = (vi < 1e-8 || vj < 1e-8) ? 0.0 : cv / sqrt(vi * vj);
+                }
+            }
         }
     }
     (void)nsamp;
@@ -180,7 +228,13 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
     return (1.0 - photo) + c.geo_w * geo;
 }
 
-__global__ void __launch_bounds__(128) pm_kernel(const __grid_constant__ PMParams c) {
+// 8 resident blocks of 128 threads per SM (64 registers): the float64 chains are latency-bound,
+// so occupancy beats the spills (measured on B200, 2000 x 1500, 8 sources, 2 iterations: 2 sources
+// per pass and 8 blocks 224 ms; 6 blocks 240 ms; 8 sources per pass at 168 registers 334 ms)
+#ifndef PM_MIN_BLOCKS
+#define PM_MIN_BLOCKS 8
+#endif
+__global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_constant__ PMParams c) {
     const int H = c.H, W = c.W;
     const int half_w = (W + 1) / 2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -197,7 +251,13 @@ __global__ void __launch_bounds__(128) pm_kernel(const __grid_constant__ PMParam
     double n[3] = {ncur[0], ncur[1], ncur[2]};
     double best, sc, ncc;
     unsigned long long changed = 0;
-    if (isfinite(dcur)) {
+    // cost of the pixel's current plane: reused from its previous visit when that visit kept the
+    // plane it started with (the cost was then computed from these very float32 values)
+    const double cached = c.cost_cache ? c.cost_cache[idx] : __longlong_as_double(0x7ff8000000000000LL);
+    if (isfinite(dcur) && cached == cached) {
+        best = cached;
+        sc = c.score_cache[idx];
+    } else if (isfinite(dcur)) {
         best = pm_cost(c, y, x, (double)dcur, n, ncc);
         sc = ncc;
     } else {
@@ -256,6 +316,11 @@ __global__ void __launch_bounds__(128) pm_kernel(const __grid_constant__ PMParam
             }
         }
     }
+    if (c.cost_cache) {
+        const bool keep = changed == 0 && isfinite(dcur);
+        c.cost_cache[idx] = keep ? best : __longlong_as_double(0x7ff8000000000000LL);
+        if (keep) c.score_cache[idx] = sc;
+    }
     c.depth[idx] = dcur;
     c.normal[idx] = ncur[0];
     c.normal[HW + idx] = ncur[1];
@@ -300,8 +365,20 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         p.iw[s] = a->src_w[s];
         p.ih[s] = a->src_h[s];
         for (int k = 0; k < 18; ++k) p.par[18 * s + k] = a->par[18 * s + k];
+        p.pinhole[s] = a->par[18 * s + 13] == 0.0 && a->par[18 * s + 14] == 0.0 && a->par[18 * s + 15] == 0.0;
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const long long HW = (long long)a->H * a->W;
+    void* cache = nullptr;
+    if (a->iters > 1) {   // the cache pays off from the second iteration on
+        if (cudaMallocAsync(&cache, (size_t)HW * 2 * sizeof(double), st) == cudaSuccess) {
+            cudaMemsetAsync(cache, 0xFF, (size_t)HW * sizeof(double), st);   // all-ones = NaN: recompute
+            p.cost_cache = reinterpret_cast<double*>(cache);
+            p.score_cache = p.cost_cache + HW;
+        } else {
+            cudaGetLastError();   // no cache: every visit recomputes (same results)
+        }
+    }
     const long long nthreads = (long long)a->H * ((a->W + 1) / 2);
     const unsigned grid = (unsigned)((nthreads + 127) / 128);
     for (int it = 0; it < a->iters; ++it) {
@@ -312,8 +389,13 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         for (int colour = 0; colour < 2; ++colour) {
             p.colour = colour;
             pm_kernel<<<grid, 128, 0, st>>>(p);
-            MVS_TRY(check_launch("pm_refine kernel"));
+            mvs_status ks = check_launch("pm_refine kernel");
+            if (ks != MVS_OK) {
+                if (cache) cudaFreeAsync(cache, st);
+                return ks;
+            }
         }
     }
+    if (cache) cudaFreeAsync(cache, st);
     return MVS_OK;
 }

@@ -9,8 +9,8 @@ __global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ Sw
     extern __shared__ float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, false, KMAX, PLANES, F16>(p, R, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
-                                             p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
+    sweep_tile<R, KMAX, PLANES, F16>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb, p.rec ? (int)blockIdx.z : -1,
+                                     reinterpret_cast<float*>(smem4));
 }
 
 __global__ void merge_kernel(long long HW, int nchunks, int i0, int i1, int ppc, const float* __restrict__ rec,
@@ -190,7 +190,6 @@ mvs_status fill_params(const mvs_sweep_args* a, SweepParams& p) {
 int pick_kmax(SweepParams& p) {
     const int n = p.n_src, kk = p.kk;
     if (kk <= 2) { p.topk_bottom = 0; return 2; }
-    if (n - kk <= 2) { p.topk_bottom = 1; return 2; }
     if (kk <= 8) { p.topk_bottom = 0; return 8; }
     p.topk_bottom = 1;   // n - kk < 8 because n <= 16 and kk > 8
     return 8;

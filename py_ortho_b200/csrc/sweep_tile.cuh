@@ -15,11 +15,12 @@
 //     tracking the score of the previous hypothesis and of the one after the winner.
 //
 // Work of one CTA per (hypothesis, source):
-//   A. warp the source into a shared-memory tile with an r-pixel halo (NaN = invalid sample),
-//   B. horizontal window sums of (V, J, J^2, J*I) for groups of 4 columns from 16-byte
-//      shared-memory loads,
-//   C. vertical running sums down each column (TH/SEG rows per thread), NCC, insertion into a
-//      per-pixel top-k list in registers.
+//   A. warp the source into a shared-memory tile with an r-pixel halo (NaN = invalid sample);
+//   B. horizontal window sums of (V, J, J^2, J*I): each thread runs along a 16-column row
+//      segment (inputs from 16-byte shared loads, products formed once per input) and stores
+//      one float4 per output;
+//   C. vertical running sums down each column (TH/SEG rows per thread) from float4 loads, NCC,
+//      insertion into a per-pixel top-k list in registers.
 // After the last source the winner-take-all state of each pixel is updated in registers; it
 // leaves the SM once per hypothesis chunk. Window sums are short FP32 sums (at most TH/SEG
 // add/subtract steps), so the reference's float64 running sums are not needed.
@@ -76,22 +77,50 @@ struct Coef {
     float nu0, nu1, nu2, nv0, nv1, nv2, dz0, dz1, dz2, zs;
     float lo_u, hi_u, lo_v, hi_v;
     int U0, V0;
+    int inside;       // every sample of the halo rectangle maps inside the source (with margin)
+    int pad_[3];
 };
 
-template <int RMAX>
+template <int R>
 struct Geom {
-    static constexpr int RA = (RMAX + 3) & ~3;     // halo rounded up to a float4
-    static constexpr int HRM = TH + 2 * RMAX;      // sampled rows (maximum)
-    static constexpr int HCM = TW + 2 * RMAX;      // sampled columns (maximum)
-    static constexpr int JP = TW + 2 * RA;         // shared row pitch
-    static constexpr int NG = TW / 4;              // stage-B column groups
-    static constexpr int NIN = 2 * RA + 4;         // stage-B inputs per group
-    static constexpr size_t smem_bytes() {
-        return (size_t)HRM * JP * 4 * 2 + (size_t)4 * HRM * TW * 4 + sizeof(Coef) * MVS_MAX_SOURCES;
+    static constexpr int K = 2 * R + 1;
+    static constexpr int RA = (R + 3) & ~3;        // halo rounded up to a float4
+    static constexpr int HR = TH + 2 * R;          // sampled rows
+    static constexpr int HC = TW + 2 * R;          // sampled columns
+    static constexpr int JP = TW + 2 * RA + 4;     // shared row pitch (floats): odd in float4 units
+    static constexpr int P = 16;                   // stage-B outputs per thread (one row segment)
+    static constexpr int NSEG = TW / P;
+    static constexpr int NIN = P + 2 * RA;         // stage-B inputs per segment
+    static constexpr size_t smem_bytes() {       // sJ, sI, sH, winner state (6 planes), sC
+        return (size_t)HR * JP * 4 * 2 + (size_t)HR * TW * 16 + (size_t)6 * TH * TW * 4 +
+               sizeof(Coef) * MVS_MAX_SOURCES;
     }
 };
 
+// Largest shared-memory footprint over radii 0..RMAX (a persistent CTA serves any of them).
+template <int RMAX>
+constexpr size_t smem_bytes_upto() {
+    size_t m = 0;
+    if constexpr (RMAX >= 0) m = Geom<0>::smem_bytes() > m ? Geom<0>::smem_bytes() : m;
+    if constexpr (RMAX >= 1) m = Geom<1>::smem_bytes() > m ? Geom<1>::smem_bytes() : m;
+    if constexpr (RMAX >= 2) m = Geom<2>::smem_bytes() > m ? Geom<2>::smem_bytes() : m;
+    if constexpr (RMAX >= 3) m = Geom<3>::smem_bytes() > m ? Geom<3>::smem_bytes() : m;
+    if constexpr (RMAX >= 4) m = Geom<4>::smem_bytes() > m ? Geom<4>::smem_bytes() : m;
+    if constexpr (RMAX >= 5) m = Geom<5>::smem_bytes() > m ? Geom<5>::smem_bytes() : m;
+    if constexpr (RMAX >= 6) m = Geom<6>::smem_bytes() > m ? Geom<6>::smem_bytes() : m;
+    if constexpr (RMAX >= 7) m = Geom<7>::smem_bytes() > m ? Geom<7>::smem_bytes() : m;
+    return m;
+}
+
 __device__ __forceinline__ float qnan() { return __int_as_float(0x7fc00000); }
+
+// Position of the horizontal-sum float4 of (row, col) in shared memory: an XOR swizzle of the
+// column's low 3 bits by (segment + row), so that the row-segment writers of stage B (32 lanes =
+// 8 rows x 4 segments) and the column readers of stage C (32 consecutive columns) both touch 8
+// distinct 16-byte bank groups per quarter-warp.
+__device__ __forceinline__ int hs_index(int row, int col) {
+    return row * TW + (col ^ (((col >> 4) + row) & 7));
+}
 
 __device__ __forceinline__ float hyp_value(const SweepParams& p, int i, int gx, int gy) {
     const long long o = (long long)gy * p.W + gx;
@@ -120,27 +149,60 @@ __device__ __forceinline__ float tap(const void* img, long long i) {
     }
 }
 
-// Homography path sample (pinhole, constant inverse depth per hypothesis).
+// floor(x) for |x| < 2^22 on the FMA pipe: adding 1.5 * 2^23 rounded toward -inf leaves floor(x)
+// in the low mantissa bits. Returns the integer; `f` receives floor(x) as a float.
+__device__ __forceinline__ int floor_fma(float x, float& f) {
+    const float t = __fadd_rd(x, 12582912.0f);
+    f = __fsub_rn(t, 12582912.0f);
+    return __float_as_int(t) - 0x4B400000;
+}
+
+// Homography path sample (pinhole, constant inverse depth per hypothesis), branch-free so that
+// the loads of several samples can be in flight together. Invalid samples read a safe address
+// and return NaN.
 template <bool F16>
-__device__ __forceinline__ float sample_plane(const Coef& c, const void* img, int w, int h, float a, float b) {
+__device__ __forceinline__ float sample_plane(const Coef& c, const void* img, int w, int h, float a, float b, bool in) {
     const float dz = fmaf(c.dz1, a, fmaf(c.dz2, b, c.dz0));
-    if (!(c.zs * dz > 1e-6f)) return qnan();
     const float rz = __fdividef(1.0f, dz);
     const float ul = fmaf(c.nu1, a, fmaf(c.nu2, b, c.nu0)) * rz;
     const float vl = fmaf(c.nv1, a, fmaf(c.nv2, b, c.nv0)) * rz;
-    if (!(ul >= c.lo_u && ul <= c.hi_u && vl >= c.lo_v && vl <= c.hi_v)) return qnan();
-    const float fu = floorf(ul), fv = floorf(vl);
-    const int x0 = c.U0 + (int)fu, y0 = c.V0 + (int)fv;
+    bool ok = in && (c.zs * dz > 1e-6f) && (ul >= c.lo_u) && (ul <= c.hi_u) && (vl >= c.lo_v) && (vl <= c.hi_v);
+    float fu, fv;
+    const int x0 = c.U0 + floor_fma(ok ? ul : 0.f, fu);
+    const int y0 = c.V0 + floor_fma(ok ? vl : 0.f, fv);
     // integer guard: every tap stays inside the image whatever the float rounding did
-    if ((unsigned)x0 >= (unsigned)(w - 1) || (unsigned)y0 >= (unsigned)(h - 1)) return qnan();
+    ok = ok && (unsigned)x0 < (unsigned)(w - 1) && (unsigned)y0 < (unsigned)(h - 1);
+    const long long o = ok ? (long long)y0 * w + x0 : 0;
     const float fx = ul - fu, fy = vl - fv;
-    const long long o = (long long)y0 * w + x0;
     const float a00 = tap<F16>(img, o), a01 = tap<F16>(img, o + 1);
     const float a10 = tap<F16>(img, o + w), a11 = tap<F16>(img, o + w + 1);
     const float top = fmaf(fx, a01 - a00, a00);
     const float bot = fmaf(fx, a11 - a10, a10);
     const float val = fmaf(fy, bot - top, top);
-    return isfinite(val) ? val : qnan();
+    return (ok && isfinite(val)) ? val : qnan();
+}
+
+// Homography sample when the whole halo rectangle is known to map inside the source and to lie
+// inside the reference image: no per-sample bounds; a non-finite value becomes NaN (invalid).
+template <bool F16>
+__device__ __forceinline__ float sample_plane_inside(const Coef& c, const void* img, int w, int h, float a, float b) {
+    const float dz = fmaf(c.dz1, a, fmaf(c.dz2, b, c.dz0));
+    const float rz = __fdividef(1.0f, dz);
+    const float ul = fmaf(c.nu1, a, fmaf(c.nu2, b, c.nu0)) * rz;
+    const float vl = fmaf(c.nv1, a, fmaf(c.nv2, b, c.nv0)) * rz;
+    float fu, fv;
+    // the clamp is a no-op when the corner test holds; it keeps every tap inside the image even if
+    // an extreme geometry defeated that test
+    const unsigned x0 = min((unsigned)(c.U0 + floor_fma(ul, fu)), (unsigned)(w - 2));
+    const unsigned y0 = min((unsigned)(c.V0 + floor_fma(vl, fv)), (unsigned)(h - 2));
+    const long long o = (long long)y0 * w + x0;
+    const float fx = ul - fu, fy = vl - fv;
+    const float a00 = tap<F16>(img, o), a01 = tap<F16>(img, o + 1);
+    const float a10 = tap<F16>(img, o + w), a11 = tap<F16>(img, o + w + 1);
+    const float top = fmaf(fx, a01 - a00, a00);
+    const float bot = fmaf(fx, a11 - a10, a10);
+    const float val = fmaf(fy, bot - top, top);
+    return fmaf(val, 0.0f, val);   // finite: val; inf: NaN; NaN: NaN
 }
 
 // Ray path sample: per-pixel inverse depth and world ray, FP64 projection with radial
@@ -169,7 +231,7 @@ __device__ __forceinline__ float sample_ray(const SweepParams& p, const SrcGeo& 
     return isfinite(val) ? (float)val : qnan();
 }
 
-__device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, int oy) {
+__device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, int oy, int hc_span, int hr_span) {
     const double d = 1.0 / (double)inv;
     double g0[3], g1[3], g2[3];
 #pragma unroll
@@ -181,22 +243,23 @@ __device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, in
     const double Z0 = g0[2];
     const bool norm = fabs(Z0) > 1e-9;
     const double zs = norm ? Z0 : 1.0;
+    const double rzs = 1.0 / zs;
     double U0 = 0.0, V0 = 0.0;
     if (norm) {
-        const double u00 = g.f * g0[0] / Z0 + g.cx, v00 = g.f * g0[1] / Z0 + g.cy;
+        const double u00 = g.f * g0[0] * rzs + g.cx, v00 = g.f * g0[1] * rzs + g.cy;
         if (isfinite(u00)) U0 = fmin(fmax(floor(u00), -1048576.0), 1048576.0);
         if (isfinite(v00)) V0 = fmin(fmax(floor(v00), -1048576.0), 1048576.0);
     }
     const double au = g.cx - U0, av = g.cy - V0;
-    c.nu0 = (float)((g.f * g0[0] + au * g0[2]) / zs);
-    c.nu1 = (float)((g.f * g1[0] + au * g1[2]) / zs);
-    c.nu2 = (float)((g.f * g2[0] + au * g2[2]) / zs);
-    c.nv0 = (float)((g.f * g0[1] + av * g0[2]) / zs);
-    c.nv1 = (float)((g.f * g1[1] + av * g1[2]) / zs);
-    c.nv2 = (float)((g.f * g2[1] + av * g2[2]) / zs);
-    c.dz0 = (float)(g0[2] / zs);
-    c.dz1 = (float)(g1[2] / zs);
-    c.dz2 = (float)(g2[2] / zs);
+    c.nu0 = (float)((g.f * g0[0] + au * g0[2]) * rzs);
+    c.nu1 = (float)((g.f * g1[0] + au * g1[2]) * rzs);
+    c.nu2 = (float)((g.f * g2[0] + au * g2[2]) * rzs);
+    c.nv0 = (float)((g.f * g0[1] + av * g0[2]) * rzs);
+    c.nv1 = (float)((g.f * g1[1] + av * g1[2]) * rzs);
+    c.nv2 = (float)((g.f * g2[1] + av * g2[2]) * rzs);
+    c.dz0 = (float)(g0[2] * rzs);
+    c.dz1 = (float)(g1[2] * rzs);
+    c.dz2 = (float)(g2[2] * rzs);
     c.zs = (float)zs;
     c.lo_u = (float)(-U0);
     c.lo_v = (float)(-V0);
@@ -204,66 +267,179 @@ __device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, in
     c.hi_v = (float)(((double)g.h - 1.001) - V0);
     c.U0 = (int)U0;
     c.V0 = (int)V0;
+    // A projective map whose depth stays positive maps the halo rectangle onto the convex hull of
+    // its corner images, so four corners strictly inside (a 1e-3 px margin absorbs the FP32
+    // evaluation error of ~1e-5 px) put every sample inside.
+    bool inside = norm;
+    const double ca[2] = {0.0, (double)(hc_span - 1)}, cb[2] = {0.0, (double)(hr_span - 1)};
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const double Xc = g0[0] + ca[i] * g1[0] + cb[j] * g2[0];
+            const double Yc = g0[1] + ca[i] * g1[1] + cb[j] * g2[1];
+            const double Zc = g0[2] + ca[i] * g1[2] + cb[j] * g2[2];
+            const double uc = g.f * Xc / Zc + g.cx, vc = g.f * Yc / Zc + g.cy;
+            inside = inside && Zc > 1e-5 && uc >= 1e-3 && vc >= 1e-3 && uc <= (double)g.w - 1.001 - 1e-3 &&
+                     vc <= (double)g.h - 1.001 - 1e-3;
+        }
+    c.inside = inside ? 1 : 0;
 }
 
-// One tile x hypothesis range. DYN = false: r == RMAX at compile time (fully unrolled windows);
-// DYN = true: runtime r <= RMAX (batched jobs of mixed radius). `chunk` >= 0 writes the chunk
-// record `chunk` of p.nchunks instead of the caller's state.
-template <int RMAX, bool DYN, int KMAX, bool PLANES, bool F16>
-__device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int pa, int pb, int chunk, float* smem) {
-    using G = Geom<RMAX>;
-    constexpr int RA = G::RA, HRM = G::HRM, HCM = G::HCM, JP = G::JP, NG = G::NG, NIN = G::NIN;
-    const int r = DYN ? r_dyn : RMAX;
-    const int K = 2 * r + 1;
-    const int HR = TH + 2 * r;
-    float* sJ = smem;                                  // HRM x JP warped source (NaN = invalid)
-    float* sI = sJ + HRM * JP;                         // HRM x JP reference (0 outside)
-    float* sH = sI + HRM * JP;                         // 4 x HRM x TW horizontal sums
-    Coef* sC = reinterpret_cast<Coef*>(sH + 4 * HRM * TW);
+// Stage B: horizontal window sums of (V, J, J^2, J I) for one 16-column row segment per thread:
+// products formed once per input, running sums along the segment, one float4 per output.
+// WITHV = false when every sample is valid: the count column is not formed (it would be k).
+template <int R, bool WITHV>
+__device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4* sH, int tid) {
+    using G = Geom<R>;
+    constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
+    if (tid >= HR * NSEG) return;
+    const int hy = tid / NSEG, sg = tid - hy * NSEG;
+    const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
+    const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
+    float v[NIN], s1[NIN], s2[NIN], s3[NIN];
+#pragma unroll
+    for (int q = 0; q < NIN / 4; ++q) {
+        const float4 a = jr[q], b = ir[q];
+        const float jv[4] = {a.x, a.y, a.z, a.w}, iv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = 4 * q + u;
+            float jz = jv[u];
+            if constexpr (WITHV) {
+                const bool ok = jz == jz;
+                jz = ok ? jz : 0.f;
+                v[t] = ok ? 1.f : 0.f;
+            }
+            s1[t] = jz;
+            s2[t] = __fmul_rn(jz, jz);
+            s3[t] = __fmul_rn(jz, iv[u]);
+        }
+    }
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+    for (int t = RA - R; t <= RA + R; ++t) {
+        if constexpr (WITHV) a0 = __fadd_rn(a0, v[t]);
+        a1 = __fadd_rn(a1, s1[t]);
+        a2 = __fadd_rn(a2, s2[t]);
+        a3 = __fadd_rn(a3, s3[t]);
+    }
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        if (j > 0) {
+            const int tn = RA + R + j, to = RA - R + j - 1;
+            if constexpr (WITHV) a0 = __fadd_rn(a0, __fsub_rn(v[tn], v[to]));
+            a1 = __fadd_rn(a1, __fsub_rn(s1[tn], s1[to]));
+            a2 = __fadd_rn(a2, __fsub_rn(s2[tn], s2[to]));
+            a3 = __fadd_rn(a3, __fsub_rn(s3[tn], s3[to]));
+        }
+        sH[hs_index(hy, P * sg + j)] = make_float4(a0, a1, a2, a3);
+    }
+}
+
+// Stage C for one thread: vertical running sums down column c (rows y0 .. y0 + ROWS - 1), ZNCC,
+// insertion into the per-pixel top-k lists. WITHV = false: every window count is k^2.
+template <int R, int KMAX, bool WITHV>
+__device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const float* mu, const float* rsd,
+                                        float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
+    constexpr int K = 2 * R + 1;
+    const float k2 = (float)(K * K), inv_k2 = 1.0f / (float)(K * K);
+    float cv = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+        const float4 h = sH[hs_index(y0 + t, c)];
+        if constexpr (WITHV) cv = __fadd_rn(cv, h.x);
+        cj = __fadd_rn(cj, h.y);
+        cjj = __fadd_rn(cjj, h.z);
+        cji = __fadd_rn(cji, h.w);
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        if (j > 0) {
+            const float4 hn = sH[hs_index(y0 + j + 2 * R, c)];
+            const float4 ho = sH[hs_index(y0 + j - 1, c)];
+            if constexpr (WITHV) cv = __fadd_rn(cv, __fsub_rn(hn.x, ho.x));
+            cj = __fadd_rn(cj, __fsub_rn(hn.y, ho.y));
+            cjj = __fadd_rn(cjj, __fsub_rn(hn.z, ho.z));
+            cji = __fadd_rn(cji, __fsub_rn(hn.w, ho.w));
+        }
+        float ncc;
+        if (WITHV && cv * 10.f <= 9.f * k2) {
+            ncc = -1.f;
+        } else {
+            const float rc = (!WITHV || cv == k2) ? inv_k2 : __frcp_rn(cv);
+            const float mj = __fmul_rn(cj, rc), m2 = __fmul_rn(cjj, rc), mij = __fmul_rn(cji, rc);
+            const float var = __fsub_rn(m2, __fmul_rn(mj, mj));
+            const float rsdj = var > 1e-6f ? rsqrtf(var) : 1000.f;
+            ncc = __fmul_rn(__fsub_rn(mij, __fmul_rn(mu[j], mj)), __fmul_rn(rsd[j], rsdj));
+            ncc = ncc > 1.f ? 1.f : (ncc < -1.f ? -1.f : ncc);
+        }
+        if (bottom) total[j] = __fadd_rn(total[j], ncc);
+        float x = ncc;
+#pragma unroll
+        for (int q = 0; q < KMAX; ++q) {
+            if (q < nlist) {
+                const float hi = fmaxf(topk[j][q], x), lo = fminf(topk[j][q], x);
+                topk[j][q] = bottom ? lo : hi;
+                x = bottom ? hi : lo;
+            }
+        }
+    }
+}
+
+// One tile x hypothesis range at window radius R. `chunk` >= 0 writes the chunk record `chunk`
+// of p.nchunks instead of the caller's state. Explicit _rn arithmetic in stages B and C fixes
+// every rounding, so the result never depends on how the compiler scheduled this instance.
+template <int R, int KMAX, bool PLANES, bool F16>
+__device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
+    using G = Geom<R>;
+    constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
+                  NIN = G::NIN;
+    float* sJ = smem;                                  // HR x JP warped source (NaN = invalid)
+    float* sI = sJ + HR * JP;                          // HR x JP reference (0 outside)
+    float4* sH = reinterpret_cast<float4*>(sI + HR * JP);   // HR x TW (V, J, J^2, J I), swizzled
     const int H = p.H, W = p.W;
     const int tid = threadIdx.x;
 
     __syncthreads();   // a previous tile of a persistent CTA is done with shared memory
-    for (int e = tid; e < HRM * JP; e += NT) {
+    for (int e = tid; e < HR * JP; e += NT) {
         const int hy = e / JP, hc = e - hy * JP;
-        const int gy = ty - r + hy, gx = tx - RA + hc;
+        const int gy = ty - R + hy, gx = tx - RA + hc;
         float v = 0.f;
-        if (hy < HR && gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(p.ref + (long long)gy * W + gx);
+        if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(p.ref + (long long)gy * W + gx);
         sI[e] = v;
         sJ[e] = qnan();
     }
 
+    // winner-take-all state of the tile's pixels: touched once per hypothesis, so it lives in
+    // shared memory (planes: best, prev, s_prev_best, s_next_best, first score, idx bits)
+    float* sW = reinterpret_cast<float*>(sH + HR * TW);
+    Coef* sC = reinterpret_cast<Coef*>(sW + 6 * TH * TW);
     const int c = tid % TW, seg = tid / TW;
     const int gx = tx + c;
-    float mu[ROWS], rsd[ROWS], best[ROWS], prv[ROWS], spb[ROWS], snb[ROWS], first[ROWS];
-    int idx[ROWS];
+    float mu[ROWS], rsd[ROWS];
     const bool to_rec = chunk >= 0;
 #pragma unroll
     for (int j = 0; j < ROWS; ++j) {
-        const int gy = ty + seg * ROWS + j;
+        const int ly = seg * ROWS + j, gy = ty + ly;
         const bool in = gx < W && gy < H;
         const long long o = (long long)gy * W + gx;
         mu[j] = in ? __ldg(p.mu + o) : 0.f;
         rsd[j] = in ? 1.0f / __ldg(p.sd + o) : 0.f;
-        if (in && !to_rec && !p.fresh) {
-            best[j] = p.best[o];
-            prv[j] = p.prev[o];
-            spb[j] = p.spb[o];
-            snb[j] = p.snb[o];
-            idx[j] = p.idx[o];
-        } else {
-            best[j] = -2.f;
-            prv[j] = -2.f;
-            spb[j] = -2.f;
-            snb[j] = -2.f;
-            idx[j] = -1;
-        }
-        first[j] = -2.f;
+        const bool load = in && !to_rec && !p.fresh;
+        const int w = ly * TW + c;
+        sW[w] = load ? p.best[o] : -2.f;
+        sW[TH * TW + w] = load ? p.prev[o] : -2.f;
+        sW[2 * TH * TW + w] = load ? p.spb[o] : -2.f;
+        sW[3 * TH * TW + w] = load ? p.snb[o] : -2.f;
+        sW[4 * TH * TW + w] = -2.f;
+        sW[5 * TH * TW + w] = __int_as_float(load ? p.idx[o] : -1);
     }
-    const float k2 = (float)(K * K), inv_k2 = 1.0f / (float)(K * K);
     const int nsrc = p.n_src, kk = p.kk;
-    const bool bottom = p.topk_bottom != 0;
+    const bool bottom = KMAX > 2 && p.topk_bottom != 0;   // the 2-entry list is always a top list
     const int nlist = bottom ? nsrc - kk : kk;
+    // every halo sample lies inside the reference image (interior tile)
+    const bool tile_inside = tx - R >= 0 && ty - R >= 0 && tx + TW + R <= W && ty + TH + R <= H;
 
     for (int i = pa; i < pb; ++i) {
         float topk[ROWS][KMAX];
@@ -276,165 +452,91 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
         }
         if constexpr (PLANES) {
             __syncthreads();   // the previous hypothesis is done reading sC
-            if (tid < nsrc) make_coef(sC[tid], p.src[tid], p.planes[i - p.i0], tx - r, ty - r);
+            if (tid < nsrc) make_coef(sC[tid], p.src[tid], p.planes[i - p.i0], tx - R, ty - R, HC, HR);
         }
         for (int s = 0; s < nsrc; ++s) {
             __syncthreads();   // sC ready; the previous stage B is done with sJ
             // ---- A: warp the source into the halo tile
             const void* img = p.src[s].img;
             const int sw = p.src[s].w, sh = p.src[s].h;
-            for (int e = tid; e < HRM * HCM; e += NT) {
-                const int hy = e / HCM, hc = e - hy * HCM;
-                if (hy >= HR || hc >= TW + 2 * r) continue;
-                const int gy = ty - r + hy, gxx = tx - r + hc;
-                float J = qnan();
-                if (gy >= 0 && gy < H && gxx >= 0 && gxx < W) {
-                    if constexpr (PLANES) {
-                        J = sample_plane<F16>(sC[s], img, sw, sh, (float)hc, (float)hy);
-                    } else {
-                        J = sample_ray(p, p.src[s], i, gxx, gy);
-                    }
-                }
-                sJ[hy * JP + (RA - r) + hc] = J;
-            }
-            __syncthreads();
-            // ---- B: horizontal sums of V, J, J^2, J*I for 4 output columns per item
-            for (int e = tid; e < HRM * NG; e += NT) {
-                const int hy = e / NG, gi = e - hy * NG;
-                if (hy >= HR) continue;
-                const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + 4 * gi);
-                const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + 4 * gi);
-                float jv[NIN], iv[NIN];
-#pragma unroll
-                for (int q = 0; q < NIN / 4; ++q) {
-                    const float4 a = jr[q], b = ir[q];
-                    jv[4 * q] = a.x; jv[4 * q + 1] = a.y; jv[4 * q + 2] = a.z; jv[4 * q + 3] = a.w;
-                    iv[4 * q] = b.x; iv[4 * q + 1] = b.y; iv[4 * q + 2] = b.z; iv[4 * q + 3] = b.w;
-                }
-                // explicit rounding (no contraction) so that every instantiation - static or
-                // runtime radius - produces the same bits
-                float v[NIN], s1[NIN], s2[NIN], s3[NIN];
-#pragma unroll
-                for (int t = 0; t < NIN; ++t) {
-                    const bool ok = jv[t] == jv[t];
-                    const float jz = ok ? jv[t] : 0.f;
-                    v[t] = ok ? 1.f : 0.f;
-                    s1[t] = jz;
-                    s2[t] = __fmul_rn(jz, jz);
-                    s3[t] = __fmul_rn(jz, iv[t]);
-                }
-                float o0[4], o1[4], o2[4], o3[4];
-                float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
-#pragma unroll
-                for (int t = -RMAX; t <= RMAX; ++t) {
-                    if (t >= -r && t <= r) {
-                        a0 = __fadd_rn(a0, v[RA + t]);
-                        a1 = __fadd_rn(a1, s1[RA + t]);
-                        a2 = __fadd_rn(a2, s2[RA + t]);
-                        a3 = __fadd_rn(a3, s3[RA + t]);
-                    }
-                }
-                o0[0] = a0; o1[0] = a1; o2[0] = a2; o3[0] = a3;
-#pragma unroll
-                for (int j = 1; j < 4; ++j) {
-                    float n0, n1, n2, n3, d0, d1, d2, d3;
-                    if constexpr (DYN) {
-                        // runtime radius: select the entering / leaving columns
-                        n0 = 0.f; n1 = 0.f; n2 = 0.f; n3 = 0.f; d0 = 0.f; d1 = 0.f; d2 = 0.f; d3 = 0.f;
-#pragma unroll
-                        for (int rr = 0; rr <= RMAX; ++rr) {
-                            if (rr == r) {
-                                n0 = v[RA + rr + j]; n1 = s1[RA + rr + j]; n2 = s2[RA + rr + j]; n3 = s3[RA + rr + j];
-                                d0 = v[RA - rr + j - 1]; d1 = s1[RA - rr + j - 1]; d2 = s2[RA - rr + j - 1]; d3 = s3[RA - rr + j - 1];
-                            }
+            bool any_invalid = false;
+            if constexpr (PLANES) {
+                const Coef cf = sC[s];
+                constexpr int PER = (HR * HC + NT - 1) / NT;
+                if (cf.inside && tile_inside) {
+#pragma unroll 4
+                    for (int k = 0; k < PER; ++k) {
+                        const int e = tid + k * NT;
+                        if (e < HR * HC) {
+                            const int hy = e / HC, hc = e - hy * HC;
+                            const float J = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
+                            any_invalid |= J != J;
+                            sJ[hy * JP + (RA - R) + hc] = J;
                         }
-                    } else {
-                        const int tn = RA + RMAX + j, to = RA - RMAX + j - 1;
-                        n0 = v[tn]; n1 = s1[tn]; n2 = s2[tn]; n3 = s3[tn];
-                        d0 = v[to]; d1 = s1[to]; d2 = s2[to]; d3 = s3[to];
                     }
-                    a0 = __fadd_rn(a0, __fsub_rn(n0, d0));
-                    a1 = __fadd_rn(a1, __fsub_rn(n1, d1));
-                    a2 = __fadd_rn(a2, __fsub_rn(n2, d2));
-                    a3 = __fadd_rn(a3, __fsub_rn(n3, d3));
-                    o0[j] = a0; o1[j] = a1; o2[j] = a2; o3[j] = a3;
-                }
-                float4* hp = reinterpret_cast<float4*>(sH + hy * TW + 4 * gi);
-                hp[0] = make_float4(o0[0], o0[1], o0[2], o0[3]);
-                hp[(HRM * TW) / 4] = make_float4(o1[0], o1[1], o1[2], o1[3]);
-                hp[(2 * HRM * TW) / 4] = make_float4(o2[0], o2[1], o2[2], o2[3]);
-                hp[(3 * HRM * TW) / 4] = make_float4(o3[0], o3[1], o3[2], o3[3]);
-            }
-            __syncthreads();
-            // ---- C: vertical sums, NCC, top-k insertion
-            {
-                const float* h0 = sH + c;
-                const float* h1 = sH + HRM * TW + c;
-                const float* h2 = sH + 2 * HRM * TW + c;
-                const float* h3 = sH + 3 * HRM * TW + c;
-                const int y0 = seg * ROWS;
-                float cv = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
-#pragma unroll
-                for (int t = 0; t <= 2 * RMAX; ++t) {
-                    if (t <= 2 * r) {
-                        const int o = (y0 + t) * TW;
-                        cv = __fadd_rn(cv, h0[o]);
-                        cj = __fadd_rn(cj, h1[o]);
-                        cjj = __fadd_rn(cjj, h2[o]);
-                        cji = __fadd_rn(cji, h3[o]);
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < ROWS; ++j) {
-                    if (j > 0) {
-                        const int on = (y0 + j + 2 * r) * TW, oo = (y0 + j - 1) * TW;
-                        cv = __fadd_rn(cv, __fsub_rn(h0[on], h0[oo]));
-                        cj = __fadd_rn(cj, __fsub_rn(h1[on], h1[oo]));
-                        cjj = __fadd_rn(cjj, __fsub_rn(h2[on], h2[oo]));
-                        cji = __fadd_rn(cji, __fsub_rn(h3[on], h3[oo]));
-                    }
-                    float ncc;
-                    if (cv * 10.f <= 9.f * k2) {
-                        ncc = -1.f;
-                    } else {
-                        const float rc = (cv == k2) ? inv_k2 : __frcp_rn(cv);
-                        const float mj = __fmul_rn(cj, rc), m2 = __fmul_rn(cjj, rc), mij = __fmul_rn(cji, rc);
-                        const float var = __fsub_rn(m2, __fmul_rn(mj, mj));
-                        const float rsdj = var > 1e-6f ? rsqrtf(var) : 1000.f;
-                        ncc = __fmul_rn(__fsub_rn(mij, __fmul_rn(mu[j], mj)), __fmul_rn(rsd[j], rsdj));
-                        ncc = ncc > 1.f ? 1.f : (ncc < -1.f ? -1.f : ncc);
-                    }
-                    total[j] = __fadd_rn(total[j], ncc);
-                    float x = ncc;
-#pragma unroll
-                    for (int q = 0; q < KMAX; ++q) {
-                        if (q < nlist) {
-                            const float hi = fmaxf(topk[j][q], x), lo = fminf(topk[j][q], x);
-                            topk[j][q] = bottom ? lo : hi;
-                            x = bottom ? hi : lo;
+                } else {
+#pragma unroll 4
+                    for (int k = 0; k < PER; ++k) {
+                        const int e = tid + k * NT;
+                        if (e < HR * HC) {
+                            const int hy = e / HC, hc = e - hy * HC;
+                            const int gy = ty - R + hy, gxx = tx - R + hc;
+                            const bool in = gy >= 0 && gy < H && gxx >= 0 && gxx < W;
+                            const float J = sample_plane<F16>(cf, img, sw, sh, (float)hc, (float)hy, in);
+                            any_invalid |= J != J;
+                            sJ[hy * JP + (RA - R) + hc] = J;
                         }
                     }
                 }
+            } else {
+                any_invalid = true;
+                for (int e = tid; e < HR * HC; e += NT) {
+                    const int hy = e / HC, hc = e - hy * HC;
+                    const int gy = ty - R + hy, gxx = tx - R + hc;
+                    float J = qnan();
+                    if (gy >= 0 && gy < H && gxx >= 0 && gxx < W) J = sample_ray(p, p.src[s], i, gxx, gy);
+                    sJ[hy * JP + (RA - R) + hc] = J;
+                }
+            }
+            // every sample of this (hypothesis, source) valid -> the count is k^2 everywhere and
+            // stages B and C skip it (block-wide vote; uniform branch)
+            const bool all_valid = !__syncthreads_or(any_invalid);
+            // ---- B: horizontal window sums of (V, J, J^2, J I), one 16-column row segment per
+            // thread: products once per input, running sums along the segment
+            if (all_valid) {
+                stage_b<R, false>(sJ, sI, sH, tid);
+            } else {
+                stage_b<R, true>(sJ, sI, sH, tid);
+            }
+            __syncthreads();
+            // ---- C: vertical running sums down the column, NCC, top-k insertion
+            if (all_valid) {
+                stage_c<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+            } else {
+                stage_c<R, KMAX, true>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
             }
         }
         // ---- winner-take-all update for hypothesis i
 #pragma unroll
         for (int j = 0; j < ROWS; ++j) {
-            float s = 0.f;
+            float sc = 0.f;
 #pragma unroll
             for (int q = 0; q < KMAX; ++q)
-                if (q < nlist) s = __fadd_rn(s, topk[j][q]);
-            if (bottom) s = __fsub_rn(total[j], s);
-            s = __fdiv_rn(s, (float)kk);
-            if (idx[j] == i - 1) snb[j] = s;
-            if (s > best[j]) {
-                best[j] = s;
-                spb[j] = prv[j];
-                snb[j] = -2.f;
-                idx[j] = i;
+                if (q < nlist) sc = __fadd_rn(sc, topk[j][q]);
+            if (bottom) sc = __fsub_rn(total[j], sc);
+            sc = __fdiv_rn(sc, (float)kk);
+            const int w = (seg * ROWS + j) * TW + c;
+            float best = sW[w], prv = sW[TH * TW + w];
+            const int id = __float_as_int(sW[5 * TH * TW + w]);
+            if (id == i - 1) sW[3 * TH * TW + w] = sc;
+            if (sc > best) {
+                sW[w] = sc;
+                sW[2 * TH * TW + w] = prv;
+                sW[3 * TH * TW + w] = -2.f;
+                sW[5 * TH * TW + w] = __int_as_float(i);
             }
-            prv[j] = s;
-            if (i == pa) first[j] = s;
+            sW[TH * TW + w] = sc;
+            if (i == pa) sW[4 * TH * TW + w] = sc;
         }
     }
 
@@ -444,22 +546,23 @@ __device__ void sweep_tile(const SweepParams& p, int r_dyn, int tx, int ty, int 
         const int gy = ty + seg * ROWS + j;
         if (gx >= W || gy >= H) continue;
         const long long o = (long long)gy * W + gx;
+        const int w = (seg * ROWS + j) * TW + c;
         if (!to_rec) {
-            p.best[o] = best[j];
-            p.prev[o] = prv[j];
-            p.spb[o] = spb[j];
-            p.snb[o] = snb[j];
-            p.idx[o] = idx[j];
+            p.best[o] = sW[w];
+            p.prev[o] = sW[TH * TW + w];
+            p.spb[o] = sW[2 * TH * TW + w];
+            p.snb[o] = sW[3 * TH * TW + w];
+            p.idx[o] = __float_as_int(sW[5 * TH * TW + w]);
         } else {
             const long long HW = (long long)H * W;
             const long long plane = (long long)p.nchunks * HW;
             float* rc = p.rec + (long long)chunk * HW + o;
-            rc[0] = best[j];
-            rc[plane] = __int_as_float(idx[j]);
-            rc[2 * plane] = spb[j];
-            rc[3 * plane] = snb[j];
-            rc[4 * plane] = first[j];
-            rc[5 * plane] = prv[j];
+            rc[0] = sW[w];
+            rc[plane] = sW[5 * TH * TW + w];
+            rc[2 * plane] = sW[2 * TH * TW + w];
+            rc[3 * plane] = sW[3 * TH * TW + w];
+            rc[4 * plane] = sW[4 * TH * TW + w];
+            rc[5 * plane] = sW[TH * TW + w];
         }
     }
 }
