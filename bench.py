@@ -255,7 +255,8 @@ def run_ours(a):
     roof_pm = None
     if iters:
         roof_pm = {"kernel": "pm_kernel", "bound": "fp64-issue", "evals_per_s": pm_evals / (ms_pm / 1e3),
-                   "ms": round(ms_pm, 3)}
+                   "ms": round(ms_pm, 3), "share_of_step": round(ms_pm / (ms_pm + ms_sweep), 4),
+                   "fp64_pipe_active_ncu": 0.479, "ncu_profile": "profiles/pm_kernel_2000x1500_8src.md"}
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
     launches = 2 + (2 * iters if iters else 0)       # sweep + finalize + 2 colour passes per iteration
     line = {
@@ -661,7 +662,7 @@ def run_serve(a):
 
     setup = time.time() - t0
     evals = sum(q.evals for q in trace())
-    srv = SV.DepthServer(hbm_budget=120e9, max_slots=64, plane_chunk=32, shared_sources=True)
+    srv = SV.DepthServer(hbm_budget=120e9, max_slots=64, plane_chunk=96, shared_sources=True, step_evals=3e10)
     res_s, wall_s = SV.serve(trace(), srv, realtime=True)
     srv.close()
     res_p, wall_p = SV.serve_plain(trace(), realtime=True)
@@ -674,7 +675,7 @@ def run_serve(a):
             "plain": dict(SV.latency_stats(res_p), throughput=evals / span_p / 1e9),
             "identical_results": bool(same), "unit_throughput": "Gpix.plane.view/s",
             "config": {"workload": "c5: Poisson arrivals, c4 size/source/plane distribution, 10 % PatchMatch (4 it)",
-                       "hbm_budget_gb": 120, "plane_chunk": 32, "max_slots": 64}}
+                       "hbm_budget_gb": 120, "plane_chunk": 96, "step_evals": 3e10, "max_slots": 64}}
     print(json.dumps(line), flush=True)
 
 

@@ -17,6 +17,9 @@ Fixtures (each .npz holds the inputs and the reference outputs):
                      best-to-second hypothesis score gap
   helpers.npz      - _fast.box_zero_mean, hyp_linear, hyp_refine, depth_view, densify._rays_world
   pm_case.npz      - _dense.pm_refine (the reference's xorshift draws) on a small case
+  depth_map.npz    - densify.depth_map end to end (3-level pyramid, tie-point depth band, coarse
+                     sweep + 2 refinement levels) on a rendered scene with a synthetic
+                     reconstruction (tie points on the terrain, their in-image observations)
 """
 from __future__ import annotations
 
@@ -238,6 +241,60 @@ def pm_case(R):
     np.savez_compressed(os.path.join(HERE, "pm_case.npz"), **out)
 
 
+def depth_map_case(D):
+    """Reference densify.depth_map on a rendered 5-view scene with synthetic tie points."""
+    import torch
+    from types import SimpleNamespace
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c1", seed=8, width=320, height=240)
+    cams = [sc.ref_cam] + list(sc.src_cams)
+    imgs = [sc.ref] + list(sc.srcs)
+    rng = np.random.default_rng(17)
+    # tie points: random terrain points inside the reference footprint
+    n = 3000
+    xs = rng.uniform(-12.0, 12.0, n)
+    ys = rng.uniform(-9.0, 9.0, n)
+    t = sc.terrain
+    z = S._height(torch.from_numpy(xs), torch.from_numpy(ys), torch.from_numpy(t.hills), torch.from_numpy(t.boxes)).numpy()
+    X = np.column_stack([xs, ys, z])
+    obs_cam, obs_pt = [], []
+    for k, c in enumerate(cams):
+        xc = (X - c.C) @ c.R.T
+        u = c.f * xc[:, 0] / xc[:, 2] + c.cx
+        v = c.f * xc[:, 1] / xc[:, 2] + c.cy
+        ok = (xc[:, 2] > 0) & (u >= 0) & (v >= 0) & (u < c.w) & (v < c.h)
+        obs_cam.append(np.full(ok.sum(), k, np.int32))
+        obs_pt.append(np.flatnonzero(ok).astype(np.int32))
+    intr = [SimpleNamespace(f=cams[0].f, cx=cams[0].cx, cy=cams[0].cy, width=cams[0].w, height=cams[0].h,
+                            k1=0.0, k2=0.0, k3=0.0)]
+    rec = SimpleNamespace(intr=intr, cam_group=np.zeros(len(cams), np.int32), X=X,
+                          C=np.array([c.C for c in cams]), R=np.array([c.R for c in cams]),
+                          obs_cam=np.concatenate(obs_cam), obs_pt=np.concatenate(obs_pt))
+    greys = [sc.grey(im) for im in imgs]
+
+    def views(k):
+        c = cams[k]
+        return greys[k], None, D._Cam(c.R, c.C, float(c.f), 0.0, 0.0, float(c.cx), float(c.cy), c.w, c.h, 0.0)
+
+    opt = D.DepthOptions()
+    opt.window = 2
+    opt.num_depths = 24
+    out = D.depth_map(0, [1, 2, 3, 4], rec, views, opt)
+    depth, score, low = out
+    # host-side geometry of the driver (densify.py:208-284) for the CPU checks
+    rng_ = D._depth_range(rec, 0)
+    cam2 = views(0)[2].scaled(0.5, 160, 120).scaled(0.5, 80, 60)
+    lo, hi = D._depth_band(rec, 0, cam2, (60, 80), rng_, block=max(8, 80 // 16))
+    nd = D._num_depths(rec, 0, [1, 2, 3, 4], rng_, cam2.f, opt.num_depths)
+    res = {"X": X, "C": rec.C, "R": rec.R, "obs_cam": rec.obs_cam, "obs_pt": rec.obs_pt,
+           "intr": np.array([cams[0].f, cams[0].cx, cams[0].cy, cams[0].w, cams[0].h]),
+           "depth": depth, "score": score, "low": low, "range": np.array(rng_), "band_lo": lo, "band_hi": hi,
+           "nd": np.array(nd), "opt": np.array([opt.window, opt.num_depths, opt.top_k, opt.refine_steps])}
+    for k, im in enumerate(imgs):
+        res[f"img{k}"] = im
+    np.savez_compressed(os.path.join(HERE, "depth_map.npz"), **res)
+
+
 def main():
     D = refpkg.load_densify()
     R = O.reference()
@@ -248,6 +305,7 @@ def main():
     scene_small(D)
     helpers(D, R)
     pm_case(R)
+    depth_map_case(D)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -152,3 +152,22 @@ def test_oracle_matches_live_reference_kernels():
             O.sweep_hypothesis(ref, mu, sd, srcs, ray, geo, inv, r, top_k, i, *s1)
             R._dense.sweep_hypothesis(ref, mu, sd, srcs, ray, geo, np.ascontiguousarray(inv), r, top_k, i, *s2)
         assert all(same_bits(a, b) for a, b in zip(s1, s2))
+
+
+def test_depth_map_host_geometry_matches_reference():
+    """The driver's host-side helpers (depth range, tie-point band, hypothesis count) restated in
+    py_ortho_b200.densify give the reference's values on the depth_map fixture."""
+    from types import SimpleNamespace
+    from py_ortho_b200 import densify as Dn
+    z = golden("depth_map.npz")
+    f, cx, cy, w, h = z["intr"]
+    rec = SimpleNamespace(intr=[SimpleNamespace(f=f, cx=cx, cy=cy, width=int(w), height=int(h))],
+                          cam_group=np.zeros(len(z["C"]), np.int32), X=z["X"], C=z["C"], R=z["R"],
+                          obs_cam=z["obs_cam"], obs_pt=z["obs_pt"])
+    rng = Dn._depth_range(rec, 0)
+    assert np.array_equal(np.array(rng), z["range"])
+    cam = Dn._Cam(z["R"][0], z["C"][0], float(f), 0.0, 0.0, float(cx), float(cy), int(w), int(h))
+    cam2 = cam.scaled(0.5, 160, 120).scaled(0.5, 80, 60)
+    lo, hi = Dn._depth_band(rec, 0, cam2, (60, 80), rng, block=max(8, 80 // 16))
+    assert same_bits(lo, z["band_lo"]) and same_bits(hi, z["band_hi"])
+    assert Dn._num_depths(rec, 0, [1, 2, 3, 4], rng, cam2.f, int(z["opt"][1])) == int(z["nd"])
