@@ -259,6 +259,40 @@ mvs_status mvs_server_set_job(mvs_server* s, int32_t slot, const mvs_sweep_args*
 mvs_status mvs_server_step(mvs_server* s, const int32_t* slots, const int32_t* chunks, int32_t n, void* stream);
 void mvs_server_destroy(mvs_server* s);
 
+/* ---------------------------------------------------------------- pass 2: geometric check */
+
+/* Camera rows here and in mvs_pm_args.par: R (9, world -> camera), C (3), f, k1, k2, k3, cx, cy. */
+typedef struct mvs_consistency_args {
+    int32_t H, W;
+    const float* depth;                    /* (H, W) the view's pass-1 depth map, NaN = none    */
+    const double* cam;                     /* host, 18 doubles: the view's camera row           */
+    int32_t n_nb, pad_;
+    const float* nb_depth[MVS_MAX_SOURCES];   /* neighbours' pass-1 depth maps (device)         */
+    int32_t nb_h[MVS_MAX_SOURCES], nb_w[MVS_MAX_SOURCES];
+    const double* nb_cam;                  /* host, n_nb x 18 camera rows                       */
+    const double* rel_tol;                 /* host, n_nb relative depth tolerances              */
+    double px_tol;                         /* forward-backward reprojection tolerance, pixels   */
+    int16_t* count;                        /* out (H, W) agreeing neighbours, or NULL           */
+    const float* grey;                     /* (H, W) grey (NaN = masked), or NULL: no mask      */
+    const float* score;                    /* (H, W) pass-1 NCC score                           */
+    double min_ncc;                        /* compared in float32                               */
+    int32_t min_views, pad2_;
+    uint8_t* active;                       /* out (H, W) PatchMatch selection, or NULL          */
+} mvs_consistency_args;
+
+/* Replaces densify._consistency (densify.py:441-478, with _fast.ref_points / neighbour_sample /
+ * agreement, _fast.pyx:201-268): per finite pixel, the number of neighbours whose depth map
+ * agrees under forward-backward reprojection. With `grey`, also pass 2's PatchMatch mask
+ * (densify.py:621): finite(grey) & (count < min_views - 1 | score < min_ncc | !finite(depth)).
+ * Bit-exact with the reference, whose 3 x 3 products NumPy evaluates as fused multiply-add
+ * chains (a = m0 r0; a = fma(m1, r1, a); a = fma(m2, r2, a)). */
+mvs_status mvs_consistency(const mvs_consistency_args* args, void* stream);
+
+/* Replaces densify._init_normals (densify.py:481-496): (3, H, W) float32 world normals of a depth
+ * map from 2-px central differences, (0, 0, 1) where undefined, facing the camera. Bit-exact. */
+mvs_status mvs_init_normals(int32_t H, int32_t W, const float* depth, const float* ray, float* normal,
+                            void* stream);
+
 /* ---------------------------------------------------------------- misc */
 
 /* Message of this thread's last failing call ("" if none). Returns the message length. */

@@ -14,6 +14,8 @@
  *   oracle_pm_refine        <- _dense.pm_refine         (_dense.pyx:405-666), with either the
  *                              reference's sequential xorshift32 draws (rng = 0) or the
  *                              counter-based draws of libmvs_b200's PatchMatch (rng = 1)
+ *   oracle_consistency      <- densify._consistency     (densify.py:441-478; _fast.pyx:201-268)
+ *   oracle_init_normals     <- densify._init_normals    (densify.py:481-496)
  * plus an all-float64 variant of the sweep (oracle_sweep_fp64) used as the precision reference:
  * every sum, NCC, score and the parabola in double, no float32 rounding anywhere.
  *
@@ -637,4 +639,178 @@ EXPORT int64_t oracle_pm_refine(int H, int W, const float* ref, const float* ray
         }
     }
     return changed;
+}
+
+/* ------------------------------------------------------------------ pass-2 geometry (densify.py:441-496) */
+/* The 3 x 3 products of the reference's consistency check are NumPy matmuls of (n, 3) rows by a
+ * 3 x 3 matrix; NumPy hands them to OpenBLAS, whose dgemm accumulates each output as
+ * a = m0 * r0; a = fma(m1, r1, a); a = fma(m2, r2, a) (checked against NumPy on this machine). */
+static double dot3_blas(double m0, double m1, double m2, double r0, double r1, double r2)
+{
+    double a = m0 * r0;
+    a = fma(m1, r1, a);
+    return fma(m2, r2, a);
+}
+
+/* _fast._undistort (_fast.pyx:145-164) */
+static void undistort(double u, double v, const double* cam, double* xo, double* yo)
+{
+    const double f = cam[12], k1 = cam[13], k2 = cam[14], k3 = cam[15], cx = cam[16], cy = cam[17];
+    const double nx = (u - cx) / f, ny = (v - cy) / f;
+    double x = nx, y = ny, r2, d, t;
+    int it;
+    for (it = 0; it < 8; it++) {
+        r2 = x * x;
+        t = y * y;
+        r2 = r2 + t;
+        d = r2 * k3;
+        d = k2 + d;
+        d = r2 * d;
+        d = k1 + d;
+        d = r2 * d;
+        d = 1.0 + d;
+        x = nx / d;
+        y = ny / d;
+    }
+    *xo = x;
+    *yo = y;
+}
+
+/* _fast._project (_fast.pyx:167-185) */
+static void project(double xc0, double xc1, double xc2, const double* cam, double* uo, double* vo)
+{
+    const double f = cam[12], k1 = cam[13], k2 = cam[14], k3 = cam[15], cx = cam[16], cy = cam[17];
+    const double z = (xc2 >= 1e-6 || isnan(xc2)) ? xc2 : 1e-6;
+    const double x = xc0 / z, y = xc1 / z;
+    double r2 = x * x, t = y * y, d;
+    r2 = r2 + t;
+    d = r2 * k3;
+    d = k2 + d;
+    d = r2 * d;
+    d = k1 + d;
+    d = r2 * d;
+    d = 1.0 + d;
+    d = f * d;
+    t = d * x;
+    *uo = t + cx;
+    t = d * y;
+    *vo = t + cy;
+}
+
+/* densify._consistency (densify.py:441-478) through its compiled path (_fast.ref_points,
+ * neighbour_sample, agreement, _fast.pyx:201-268): per finite pixel of the reference depth map D,
+ * the number of neighbour depth maps that agree (forward-backward reprojection within px_tol
+ * pixels and relative depth within rel_tol[j]). Camera rows: R (9), C (3), f, k1, k2, k3, cx, cy.
+ * The optional active mask is pass 2's PatchMatch selection (densify.py:621):
+ * finite(grey) & ((count < min_views - 1) | (score < min_ncc) | !finite(D)), with min_ncc
+ * compared in float32 as NumPy does for a float32 array. */
+EXPORT void oracle_consistency(int H, int W, const float* D, const double* cam, int n_nb, const float* const* nb_depth,
+                               const int* nb_h, const int* nb_w, const double* nb_cam, const double* rel_tol,
+                               double px_tol, int16_t* count, const float* grey, const float* score, double min_ncc,
+                               int min_views, uint8_t* active)
+{
+    const double* R = cam;
+    const double* C = cam + 9;
+    const float min_ncc_f = (float)min_ncc;
+    int y, x, j, i;
+    for (y = 0; y < H; y++) {
+        for (x = 0; x < W; x++) {
+            const ptrdiff_t idx = (ptrdiff_t)y * W + x;
+            const float Dv = D[idx];
+            int c = 0;
+            if (isfinite(Dv)) {
+                const double d = Dv;
+                double rx, ry, M[3], X[3];
+                undistort((double)x, (double)y, cam, &rx, &ry);
+                M[0] = rx * d; M[1] = ry * d; M[2] = d;
+                for (i = 0; i < 3; i++) X[i] = C[i] + dot3_blas(M[0], M[1], M[2], R[i], R[3 + i], R[6 + i]);
+                for (j = 0; j < n_nb; j++) {
+                    const double* cj = nb_cam + 18 * j;
+                    const double* Rj = cj;
+                    const double* Cj = cj + 9;
+                    double dx[3], xc[3], u, v, dd, xj, yj, Mj[3], Xj[3], dk[3], xk[3], ub, vb;
+                    int64_t a, b;
+                    for (i = 0; i < 3; i++) dx[i] = X[i] - Cj[i];
+                    for (i = 0; i < 3; i++) xc[i] = dot3_blas(dx[0], dx[1], dx[2], Rj[3 * i], Rj[3 * i + 1], Rj[3 * i + 2]);
+                    project(xc[0], xc[1], xc[2], cj, &u, &v);
+                    a = (int64_t)rint(u);
+                    b = (int64_t)rint(v);
+                    if (xc[2] > 0 && a >= 0 && b >= 0 && a < nb_w[j] && b < nb_h[j])
+                        dd = nb_depth[j][(ptrdiff_t)b * nb_w[j] + a];
+                    else
+                        dd = NAN;
+                    undistort((double)a, (double)b, cj, &xj, &yj);
+                    Mj[0] = xj * dd; Mj[1] = yj * dd; Mj[2] = dd;
+                    for (i = 0; i < 3; i++) Xj[i] = Cj[i] + dot3_blas(Mj[0], Mj[1], Mj[2], Rj[i], Rj[3 + i], Rj[6 + i]);
+                    for (i = 0; i < 3; i++) dk[i] = Xj[i] - C[i];
+                    for (i = 0; i < 3; i++) xk[i] = dot3_blas(dk[0], dk[1], dk[2], R[3 * i], R[3 * i + 1], R[3 * i + 2]);
+                    project(xk[0], xk[1], xk[2], cam, &ub, &vb);
+                    {
+                        const double t = rel_tol[j] * dd;
+                        if (isfinite(dd) && hypot(ub - (double)x, vb - (double)y) <= px_tol && fabs(dd - xc[2]) <= t) c++;
+                    }
+                }
+            }
+            if (count) count[idx] = (int16_t)c;
+            if (active) {
+                const int fin_g = isfinite(grey[idx]);
+                active[idx] = (uint8_t)(fin_g && (c < min_views - 1 || score[idx] < min_ncc_f || !isfinite(Dv)));
+            }
+        }
+    }
+}
+
+/* densify._init_normals (densify.py:481-496), float32 NumPy semantics: P = ray * D (NaN where D is
+ * not finite), 2-px central differences along columns (tu) and rows (tv), n = tu x tv
+ * (np.cross: a1 b2 - a2 b1, ...), |n| = sqrt((n0^2 + n1^2) + n2^2), n / |n| or (0, 0, 1) where
+ * |n| is not finite or < 1e-12, negated where n . ray = (n0 r0 + n1 r1) + n2 r2 > 0. */
+EXPORT void oracle_init_normals(int H, int W, const float* D, const float* ray, float* normal)
+{
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    int y, x, k;
+    for (y = 0; y < H; y++) {
+        for (x = 0; x < W; x++) {
+            const ptrdiff_t idx = (ptrdiff_t)y * W + x;
+            float tu[3], tv[3], n[3], nn, s;
+            const float nanf_ = NAN;
+            for (k = 0; k < 3; k++) {
+                tu[k] = nanf_;
+                tv[k] = nanf_;
+            }
+            if (x >= 2 && x < W - 2) {
+                const float da = D[idx + 2], db = D[idx - 2];
+                const float pa = isfinite(da) ? da : nanf_, pb = isfinite(db) ? db : nanf_;
+                for (k = 0; k < 3; k++) tu[k] = ray[k * HW + idx + 2] * pa - ray[k * HW + idx - 2] * pb;
+            }
+            if (y >= 2 && y < H - 2) {
+                const float da = D[idx + 2 * (ptrdiff_t)W], db = D[idx - 2 * (ptrdiff_t)W];
+                const float pa = isfinite(da) ? da : nanf_, pb = isfinite(db) ? db : nanf_;
+                for (k = 0; k < 3; k++) tv[k] = ray[k * HW + idx + 2 * (ptrdiff_t)W] * pa - ray[k * HW + idx - 2 * (ptrdiff_t)W] * pb;
+            }
+            {
+                const float p0 = tu[1] * tv[2], q0 = tu[2] * tv[1];
+                const float p1 = tu[2] * tv[0], q1 = tu[0] * tv[2];
+                const float p2 = tu[0] * tv[1], q2 = tu[1] * tv[0];
+                n[0] = p0 - q0;
+                n[1] = p1 - q1;
+                n[2] = p2 - q2;
+            }
+            {
+                const float s0 = n[0] * n[0], s1 = n[1] * n[1], s2 = n[2] * n[2];
+                nn = sqrtf((s0 + s1) + s2);
+            }
+            if (!isfinite(nn) || nn < 1e-12f) {
+                n[0] = 0.0f; n[1] = 0.0f; n[2] = 1.0f;
+            } else {
+                for (k = 0; k < 3; k++) n[k] = n[k] / nn;
+            }
+            {
+                const float s0 = n[0] * ray[idx], s1 = n[1] * ray[HW + idx], s2 = n[2] * ray[2 * HW + idx];
+                s = (s0 + s1) + s2;
+            }
+            if (s > 0.0f)
+                for (k = 0; k < 3; k++) n[k] = -n[k];
+            for (k = 0; k < 3; k++) normal[k * HW + idx] = n[k];
+        }
+    }
 }

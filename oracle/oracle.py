@@ -59,6 +59,11 @@ def lib() -> C.CDLL:
                                        vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
                                        C.c_double, C.c_double, C.c_uint32, C.c_int, C.c_int]
         L.oracle_pm_uniform.restype = C.c_double
+        L.oracle_consistency.restype = None
+        L.oracle_consistency.argtypes = [C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp,
+                                         C.c_double, C.c_int, vp]
+        L.oracle_init_normals.restype = None
+        L.oracle_init_normals.argtypes = [C.c_int, C.c_int, vp, vp, vp]
         L.oracle_pm_uniform.argtypes = [C.c_uint32, C.c_int, C.c_int64, C.c_int]
         _lib = L
     return _lib
@@ -258,3 +263,43 @@ def pm_refine(ref, ray, Cr, srcs, src_depths, par, depth, normal, score, active,
 
 def pm_uniform(seed: int, it: int, pixel: int, draw: int) -> float:
     return float(lib().oracle_pm_uniform(seed & 0xFFFFFFFF, it, pixel, draw))
+
+
+# ------------------------------------------------------------------ pass-2 geometry
+def cam_row(cam) -> np.ndarray:
+    """R (9), C (3), f, k1, k2, k3, cx, cy of a densify._Cam-like camera, float64."""
+    return np.r_[np.asarray(cam.R, np.float64).ravel(), np.asarray(cam.C, np.float64), cam.f, cam.k1, cam.k2,
+                 cam.k3, cam.cx, cam.cy].astype(np.float64)
+
+
+def consistency(D, cam_r, nb_maps, nb_cams, px_tol, rel_tol, grey=None, score=None, min_ncc=0.0, min_views=0):
+    """densify._consistency (densify.py:441-478) restated: int16 agreement count per pixel; with
+    grey and score also pass 2's active mask (densify.py:621). Returns (count, active or None)."""
+    D = _f32(D)
+    H, W = D.shape
+    n = len(nb_maps)
+    maps = [_f32(m) for m in nb_maps]
+    mp = (C.c_void_p * max(n, 1))(*[m.ctypes.data for m in maps])
+    hs = np.array([m.shape[0] for m in maps] or [0], np.int32)
+    ws = np.array([m.shape[1] for m in maps] or [0], np.int32)
+    rows = _f64(np.array([cam_row(c) for c in nb_cams], np.float64).reshape(-1))
+    tol = _f64(np.asarray(rel_tol, np.float64).reshape(-1))
+    cnt = np.zeros((H, W), np.int16)
+    act = None
+    g = s = None
+    if grey is not None:
+        act = np.zeros((H, W), np.uint8)
+        g, s = _f32(grey), _f32(score)
+    lib().oracle_consistency(H, W, _p(D), _p(_f64(cam_row(cam_r))), n, mp, _p(hs), _p(ws), _p(rows), _p(tol),
+                             float(px_tol), _p(cnt), None if g is None else _p(g), None if s is None else _p(s),
+                             float(min_ncc), int(min_views), None if act is None else _p(act))
+    return cnt, act
+
+
+def init_normals(D, ray) -> np.ndarray:
+    """densify._init_normals (densify.py:481-496) restated in float32."""
+    D = _f32(D)
+    H, W = D.shape
+    out = np.empty((3, H, W), np.float32)
+    lib().oracle_init_normals(H, W, _p(D), _p(_f32(ray)), _p(out))
+    return out

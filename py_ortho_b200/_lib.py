@@ -53,6 +53,13 @@ class PMArgs(C.Structure):
                 ("seed", C.c_uint32), ("it0", i32), ("changed", vp)]
 
 
+class ConsArgs(C.Structure):
+    _fields_ = [("H", i32), ("W", i32), ("depth", vp), ("cam", vp), ("n_nb", i32), ("pad_", i32),
+                ("nb_depth", vp * MAX_SOURCES), ("nb_h", i32 * MAX_SOURCES), ("nb_w", i32 * MAX_SOURCES),
+                ("nb_cam", vp), ("rel_tol", vp), ("px_tol", C.c_double), ("count", vp), ("grey", vp),
+                ("score", vp), ("min_ncc", C.c_double), ("min_views", i32), ("pad2_", i32), ("active", vp)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("sweep", SweepArgs), ("depth", vp)]
 
@@ -86,6 +93,8 @@ SIGNATURES = {
     "mvs_server_set_job": (i32, [vp, i32, vp, vp, i32]),
     "mvs_server_step": (i32, [vp, vp, vp, i32, vp]),
     "mvs_server_destroy": (None, [vp]),
+    "mvs_consistency": (i32, [vp, vp]),
+    "mvs_init_normals": (i32, [i32, i32, vp, vp, vp, vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_version": (C.c_char_p, []),
 }

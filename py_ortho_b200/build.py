@@ -20,11 +20,13 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
           "--expt-relaxed-constexpr", "-I", INCLUDE]
-# per-file extra flags: PatchMatch is evaluated without contraction (float64, one rounding per op)
+# per-file extra flags: PatchMatch and the pass-2 geometry are evaluated without contraction
+# (one rounding per written operation, as the reference's C evaluates them)
 EXTRA = {
     "patchmatch.cu": ["-fmad=false"],
+    "views.cu": ["-fmad=false"],
 }
-SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu", "noalloc.cu"]
+SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu", "noalloc.cu", "views.cu"]
 
 
 def nvcc() -> str:

@@ -273,6 +273,16 @@ def depth_map(k, nbrs, rec, views, opt: DepthOptions):
     reference's coarse-to-fine schedule (densify.py:373-437): full sweep at 1/4 resolution over a
     per-pixel inverse-depth band, then +-refine_steps at 1/2 and full resolution. Returns
     (depth float32 with NaN, score float32, low_texture bool) as NumPy arrays, or None."""
+    out = depth_map_device(k, nbrs, rec, views, opt)
+    if out is None:
+        return None
+    depth, score, low = out
+    torch.cuda.current_stream().synchronize()
+    return depth.cpu().numpy(), score.cpu().numpy(), low.cpu().numpy()
+
+
+def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
+    """depth_map with its results left on the device: (depth, score, low_texture) tensors, or None."""
     rng = _depth_range(rec, k)
     if rng is None or not nbrs:
         return None
@@ -313,26 +323,15 @@ def depth_map(k, nbrs, rec, views, opt: DepthOptions):
                                        Hypotheses.refine(iu, dstep, opt.refine_steps), opt, rays[lvl],
                                        precision=L.PREC_FP32)
         dstep = dstep / 2
-    torch.cuda.current_stream().synchronize()
-    depth = d.cpu().numpy()
-    sd = sd.cpu().numpy() * 64.0
-    depth[ref_mask | (depth < rng[0]) | (depth > rng[1])] = np.nan
-    low_texture = sd < opt.min_texture
-    return depth, score.cpu().numpy(), low_texture
+    mask = torch.from_numpy(ref_mask).to(d.device)
+    depth = torch.where(mask | (d < rng[0]) | (d > rng[1]), torch.full_like(d, float("nan")), d)
+    low_texture = (sd * 64.0) < opt.min_texture
+    return depth, score, low_texture
 
 
 def _init_normals(D, ray):
-    """World-frame normals from 2-px central differences, facing the camera (densify.py:481-496)."""
-    P = ray * np.where(np.isfinite(D), D, np.nan)[None]
-    tu = np.full_like(P, np.nan)
-    tv = np.full_like(P, np.nan)
-    tu[:, :, 2:-2] = P[:, :, 4:] - P[:, :, :-4]
-    tv[:, 2:-2, :] = P[:, 4:, :] - P[:, :-4, :]
-    n = np.cross(tu, tv, axis=0)
-    nn = np.linalg.norm(n, axis=0)
-    bad = ~np.isfinite(nn) | (nn < 1e-12)
-    n = n / np.where(bad, 1, nn)[None]
-    n[:, bad] = np.array([0.0, 0.0, 1.0])[:, None]
-    flip = np.sum(n * ray, 0) > 0
-    n[:, flip] *= -1
-    return np.ascontiguousarray(n, np.float32)
+    """World-frame normals from 2-px central differences, facing the camera (densify.py:481-496),
+    computed on the device (mvs_init_normals); NumPy in, NumPy out."""
+    n = fast.init_normals(D, ray)
+    torch.cuda.current_stream().synchronize()
+    return n.cpu().numpy()

@@ -92,6 +92,20 @@ def rays_world(shape, cam, host: bool = False):
     return _out(out, host)
 
 
+def init_normals(D, ray) -> torch.Tensor:
+    """(3, H, W) float32 initial PatchMatch normals of depth map D (densify._init_normals,
+    densify.py:481-496) on the device, bit-identical to the reference."""
+    d_t, _ = _in(D)
+    r_t, _ = _in(ray)
+    H, W = int(d_t.shape[0]), int(d_t.shape[1])
+    if tuple(r_t.shape) != (3, H, W):
+        raise ValueError("init_normals: ray must be (3, H, W)")
+    out = torch.empty((3, H, W), dtype=torch.float32, device=d_t.device)
+    L.check(L.load().mvs_init_normals(H, W, d_t.data_ptr(), r_t.data_ptr(), out.data_ptr(), L.stream_handle()),
+            "init_normals")
+    return out
+
+
 def depth_view(rgb, gain=None, bias=None, mask=None):
     """uint8 RGB -> (grey float32 with NaN = masked, rgb8 uint8) (_fast.pyx:577-624)."""
     t, host = _in(rgb, torch.uint8)

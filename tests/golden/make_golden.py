@@ -20,10 +20,15 @@ Fixtures (each .npz holds the inputs and the reference outputs):
   depth_map.npz    - densify.depth_map end to end (3-level pyramid, tie-point depth band, coarse
                      sweep + 2 refinement levels) on a rendered scene with a synthetic
                      reconstruction (tie points on the terrain, their in-image observations)
+  views_case.npz   - densify._densify passes 1 and 2 end to end on a rendered 5-view scene
+                     (depth maps, geometric consistency, PatchMatch repair with the neighbours'
+                     depth maps, final filter), recording what the reference's own
+                     _consistency, _init_normals and _dense.pm_refine received and returned
 """
 from __future__ import annotations
 
 import os
+import shutil
 import sys
 
 import numpy as np
@@ -295,6 +300,139 @@ def depth_map_case(D):
     np.savez_compressed(os.path.join(HERE, "depth_map.npz"), **res)
 
 
+def _tie_points(sc, cams, rng, n, half_x, half_y):
+    """Random terrain points and their in-image observations (obs_cam, obs_pt)."""
+    import torch
+    from py_ortho_b200 import scene as S
+    xs = rng.uniform(-half_x, half_x, n)
+    ys = rng.uniform(-half_y, half_y, n)
+    t = sc.terrain
+    z = S._height(torch.from_numpy(xs), torch.from_numpy(ys), torch.from_numpy(t.hills), torch.from_numpy(t.boxes)).numpy()
+    X = np.column_stack([xs, ys, z])
+    obs_cam, obs_pt = [], []
+    for k, c in enumerate(cams):
+        xc = (X - c.C) @ c.R.T
+        u = c.f * xc[:, 0] / xc[:, 2] + c.cx
+        v = c.f * xc[:, 1] / xc[:, 2] + c.cy
+        ok = (xc[:, 2] > 0) & (u >= 0) & (v >= 0) & (u < c.w) & (v < c.h)
+        obs_cam.append(np.full(ok.sum(), k, np.int32))
+        obs_pt.append(np.flatnonzero(ok).astype(np.int32))
+    return X, np.concatenate(obs_cam), np.concatenate(obs_pt)
+
+
+def views_case(D, W=160, H=120):
+    """The reference's _densify, passes 1 and 2, on a rendered 5-view scene. The image loader is
+    replaced by the rendered uint8 images (grey in all three channels, so the reference's RGB mean
+    is exact); _consistency, _init_normals and _dense.pm_refine are wrapped to record their
+    arguments and results; the depth-map folder is kept and read back."""
+    import tempfile
+    import threading
+    from types import SimpleNamespace
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c1", seed=9, width=W, height=H)
+    cams = [sc.ref_cam] + list(sc.src_cams)
+    imgs = [sc.ref] + list(sc.srcs)
+    N = len(cams)
+    X, obs_cam, obs_pt = _tie_points(sc, cams, np.random.default_rng(23), 6000, 40.0, 30.0)
+    intr = [SimpleNamespace(f=float(cams[0].f), cx=float(cams[0].cx), cy=float(cams[0].cy), width=W, height=H,
+                            k1=0.0, k2=0.0, k3=0.0)]
+    rec = SimpleNamespace(used=list(range(N)), intr=intr, cam_group=np.zeros(N, np.int32), X=X,
+                          C=np.array([c.C for c in cams]), R=np.array([c.R for c in cams]), obs_cam=obs_cam,
+                          obs_pt=obs_pt, rms_px=0.5)
+    frames = [SimpleNamespace(width=W, height=H, path=f"view{k}") for k in range(N)]
+    ar = SimpleNamespace(frames=frames, workers=1)
+    rgb = {f"view{k}": np.ascontiguousarray(np.repeat(imgs[k][:, :, None], 3, axis=2)) for k in range(N)}
+    saved = (D.load_rgb, D.load_mask, D._consistency, D._init_normals, D._dense)
+    rec_cons, rec_norm, rec_pm = {}, [], {}
+    lock = threading.Lock()
+
+    def consistency(k, Dk, nbrs_k, dm, cams_, px_tol, rel_tol):
+        cnt = saved[2](k, Dk, nbrs_k, dm, cams_, px_tol, rel_tol)
+        with lock:
+            rec_cons[k] = dict(nbrs=[j for j in nbrs_k if j in dm], px_tol=float(px_tol),
+                               rel_tol=[float(rel_tol[j]) for j in nbrs_k if j in dm], cnt=cnt.copy())
+        return cnt
+
+    def init_normals(Dk, ray):
+        n = saved[3](Dk, ray)
+        with lock:
+            rec_norm.append((np.array(Dk, np.float32), n.copy()))
+        return n
+
+    class DenseProxy:
+        def __getattr__(self, name):
+            return getattr(saved[4], name)
+
+        def pm_refine(self, ref, ray, Cr, srcs, sdeps, par, depth, normal, score, active, r, step, top_k, geo_w,
+                      geo_tol, iters, dmin, dmax, seed):
+            before = dict(depth=depth.copy(), normal=normal.copy(), score=score.copy(), active=active.copy(),
+                          ref=ref.copy(), Cr=np.array(Cr), par=np.array(par),
+                          args=np.array([r, step, top_k, iters, seed], np.int64),
+                          fargs=np.array([geo_w, geo_tol, dmin, dmax], np.float64))
+            ch = saved[4].pm_refine(ref, ray, Cr, srcs, sdeps, par, depth, normal, score, active, r, step, top_k,
+                                    geo_w, geo_tol, iters, dmin, dmax, seed)
+            before.update(depth_out=depth.copy(), normal_out=normal.copy(), score_out=score.copy(),
+                          changed=np.array(ch))
+            with lock:
+                rec_pm[tuple(np.round(np.asarray(Cr, np.float64) * 1000).astype(np.int64))] = before
+            return ch
+
+    opt = D.DepthOptions()
+    opt.window, opt.num_depths, opt.patchmatch, opt.keep_depthmaps, opt.workers = 2, 24, True, True, 1
+    out_dir = tempfile.mkdtemp(prefix="views_case_")
+    D.load_rgb = lambda fr, s: rgb[fr.path]
+    D.load_mask = lambda path, w, h: None
+    D._consistency, D._init_normals, D._dense = consistency, init_normals, DenseProxy()
+    try:
+        try:
+            D.densify(ar, rec, {}, None, out_dir, opt)
+        except RuntimeError as e:                     # fusion may find too few points: not needed here
+            print("views_case: fusion:", e)
+    finally:
+        D.load_rgb, D.load_mask, D._consistency, D._init_normals, D._dense = saved
+    wd = os.path.join(out_dir, "depthmaps")
+    res = {"X": X, "C": rec.C, "R": rec.R, "obs_cam": obs_cam, "obs_pt": obs_pt, "rms_px": np.array(rec.rms_px),
+           "intr": np.array([cams[0].f, cams[0].cx, cams[0].cy, W, H]),
+           "opt": np.array([opt.window, opt.num_depths, opt.top_k, opt.refine_steps, opt.pm_iters, opt.pm_window,
+                            opt.pm_step], np.int64),
+           "fopt": np.array([opt.min_ncc, opt.min_texture, opt.pm_geo_weight], np.float64)}
+    have = []
+    for k in range(N):
+        res[f"img{k}"] = imgs[k]
+        if not os.path.exists(os.path.join(wd, f"p{k:05d}.npy")):
+            continue
+        have.append(k)
+        res[f"p{k}"] = np.load(os.path.join(wd, f"p{k:05d}.npy"))
+        res[f"s{k}"] = np.load(os.path.join(wd, f"s{k:05d}.npy"))
+        res[f"t{k}"] = np.load(os.path.join(wd, f"t{k:05d}.npy"))
+        res[f"final{k}"] = np.load(os.path.join(wd, f"{k:05d}.npy"))
+        if k in rec_cons:
+            c = rec_cons[k]
+            res[f"cnt{k}"] = c["cnt"]
+            res[f"nbrs{k}"] = np.array(c["nbrs"], np.int32)
+            res[f"tol{k}"] = np.array(c["rel_tol"], np.float64)
+            res["px_tol"] = np.array(c["px_tol"])
+    # PatchMatch: its inputs are the pass-1 maps, the images, the cameras, _init_normals of the
+    # raw map and the active mask; the outputs are kept for the first view only (size)
+    for k in have:
+        pm = rec_pm.get(tuple(np.round(np.asarray(rec.C[k], np.float64) * 1000).astype(np.int64)))
+        if pm is None:
+            continue
+        assert np.array_equal(pm["depth"], res[f"p{k}"], equal_nan=True)
+        for key in ("active", "args", "fargs", "changed"):
+            res[f"pm{k}_{key}"] = pm[key]
+        if k == have[0]:
+            for key in ("depth_out", "normal_out", "score_out"):
+                res[f"pm{k}_{key}"] = pm[key]
+    res["have"] = np.array(have, np.int32)
+    # the first recorded _init_normals call (the first repaired view's raw map), bit for bit
+    Dn, nn = rec_norm[0]
+    res["norm_view"] = np.array([k for k in have if np.array_equal(res[f"p{k}"], Dn, equal_nan=True)][0])
+    res["norm_out"] = nn
+    np.savez_compressed(os.path.join(HERE, "views_case.npz"), **res)
+    shutil.rmtree(out_dir, ignore_errors=True)
+
+
 def main():
     D = refpkg.load_densify()
     R = O.reference()
@@ -306,6 +444,7 @@ def main():
     helpers(D, R)
     pm_case(R)
     depth_map_case(D)
+    views_case(D)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -1,0 +1,106 @@
+"""Pass 2 on the device against the reference (views_case.npz): the consistency count and the
+PatchMatch mask (mvs_consistency) and the initial normals (mvs_init_normals) bit for bit, the
+pass-2 PatchMatch repair bit for bit against the oracle with the same counter-based draws, and
+passes 1 + 2 end to end (py_ortho_b200.views.densify_views) against the reference's final
+depth maps."""
+import numpy as np
+import pytest
+import torch
+
+from conftest import same_bits
+from tests_support import views_fixture
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def test_consistency_and_mask_match_reference():
+    from py_ortho_b200 import views as V
+    z, rec, cams, greys = views_fixture()
+    mn = float(z["fopt"][0])
+    for k in z["have"]:
+        nb = list(z[f"nbrs{k}"])
+        S = z[f"s{k}"].astype(np.float32)
+        cnt, act = V.consistency(_dev(z[f"p{k}"]), cams[k], [_dev(z[f"p{j}"]) for j in nb], [cams[j] for j in nb],
+                                 float(z["px_tol"]), z[f"tol{k}"], grey=_dev(greys[k]), score=_dev(S), min_ncc=mn,
+                                 min_views=3)
+        assert np.array_equal(cnt.cpu().numpy(), z[f"cnt{k}"]), k
+        assert np.array_equal(act.cpu().numpy(), z[f"pm{k}_active"]), k
+        # the reference-signature drop-in (NumPy in, NumPy out)
+        dm = {j: z[f"p{j}"] for j in z["have"]}
+        tol = dict(zip(nb, z[f"tol{k}"]))
+        assert np.array_equal(V._consistency(k, z[f"p{k}"], nb, dm, cams, float(z["px_tol"]), tol), z[f"cnt{k}"])
+
+
+def test_init_normals_match_reference():
+    from py_ortho_b200 import fast
+    from py_ortho_b200.densify import _init_normals
+    z, rec, cams, greys = views_fixture()
+    k = int(z["norm_view"])
+    H, W = greys[k].shape
+    ray = fast.rays_world((H, W), cams[k])
+    n = fast.init_normals(_dev(z[f"p{k}"]), ray)
+    assert same_bits(n.cpu().numpy(), z["norm_out"])
+    assert same_bits(_init_normals(z[f"p{k}"], ray.cpu().numpy()), z["norm_out"])
+
+
+def test_pass2_patchmatch_matches_oracle():
+    """The device repair of one view (geometric term on the neighbours' maps) against the oracle
+    with the same counter-based draws: bit-identical depth, normal, score and change count."""
+    from oracle import oracle as O
+    from py_ortho_b200 import dense, fast
+    z, rec, cams, greys = views_fixture()
+    k = int(z["have"][0])
+    nb = list(z[f"nbrs{k}"])
+    r, step, top_k, iters, seed = (int(v) for v in z[f"pm{k}_args"])
+    gw, gt, dmin, dmax = (float(v) for v in z[f"pm{k}_fargs"])
+    H, W = greys[k].shape
+    ray = fast.rays_world((H, W), cams[k]).cpu().numpy()
+    par = np.array([O.cam_row(cams[j]) for j in nb])
+    act = z[f"pm{k}_active"]
+    D0 = z[f"p{k}"].copy()
+    N0 = O.init_normals(D0, ray)
+    S0 = z[f"s{k}"].astype(np.float32)
+    Do, No, So = D0.copy(), N0.copy(), S0.copy()
+    ch_o = O.pm_refine(greys[k], ray, cams[k].C, [greys[j] for j in nb], [z[f"p{j}"] for j in nb], par, Do, No, So,
+                       act, r, step, top_k, gw, gt, iters, dmin, dmax, seed, rng=1)
+    Dg, Ng, Sg = _dev(D0), _dev(N0), _dev(S0)
+    ch_g = dense.pm_refine(_dev(greys[k]), _dev(ray), cams[k].C, [_dev(greys[j]) for j in nb],
+                           [_dev(z[f"p{j}"]) for j in nb], par, Dg, Ng, Sg, _dev(act), r, step, top_k, gw, gt,
+                           iters, dmin, dmax, seed)
+    assert ch_g == ch_o and ch_o > 0
+    assert same_bits(Dg.cpu().numpy(), Do) and same_bits(Ng.cpu().numpy(), No) and same_bits(Sg.cpu().numpy(), So)
+
+
+def test_densify_views_end_to_end_against_reference():
+    """Passes 1 and 2 on the device against the reference's final depth maps. PatchMatch runs a
+    red-black schedule with counter-based draws where the reference visits pixels in raster order
+    with one xorshift stream, so repaired pixels agree statistically, not bit for bit."""
+    from py_ortho_b200 import views as V
+    from py_ortho_b200.densify import DepthOptions, _Cam
+    z, rec, cams_ns, greys = views_fixture()
+    cams = [_Cam(c.R, c.C, c.f, 0.0, 0.0, c.cx, c.cy, c.w, c.h) for c in cams_ns]
+    opt = DepthOptions()
+    opt.window, opt.num_depths = int(z["opt"][0]), int(z["opt"][1])
+    opt.patchmatch = True
+
+    def views(k):
+        return greys[k], None, cams[k]
+
+    out = V.densify_views(rec, views, opt)
+    assert sorted(out) == sorted(int(k) for k in z["have"])
+    for k, (D, ch, na) in sorted(out.items()):
+        ref = z[f"final{k}"]
+        fin, rfin = np.isfinite(D), np.isfinite(ref)
+        both = fin & rfin
+        rel = np.abs(D[both].astype(np.float64) - ref[both]) / ref[both]
+        print(f"view {k}: finite agree {(fin == rfin).mean():.4f}, median rel {np.median(rel):.2e}, "
+              f"<=0.1% {(rel <= 1e-3).mean():.4f}, PM changes {ch}, active {na}")
+        ref_na = int(z[f"pm{k}_active"].sum())             # the mask follows pass 1's near-ties
+        assert abs(na - ref_na) <= 0.05 * ref_na
+        assert (fin == rfin).mean() > 0.95
+        assert np.median(rel) < 1e-3
+        assert (rel <= 1e-3).mean() > 0.8

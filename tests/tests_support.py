@@ -74,3 +74,22 @@ def check_parity(idx, depth, best, ref_idx, ref_depth, ref_best, gap, label=""):
         assert e.size == 0 or e.max() <= SCORE_ABS, f"{label}: score error {e.max():.3e}"
         out["score_abs_max"] = float(e.max()) if e.size else 0.0
     return out
+
+
+def views_fixture():
+    """views_case.npz (the reference's passes 1 and 2 on a rendered 5-view scene) unpacked:
+    (z, rec, cams, greys) with densify._Cam-like cameras at matching scale."""
+    from types import SimpleNamespace as NS
+    from conftest import golden
+    z = golden("views_case.npz")
+    f, cx, cy, W, H = z["intr"]
+    N = len(z["C"])
+    cams = [NS(R=z["R"][k], C=z["C"][k], f=float(f), k1=0.0, k2=0.0, k3=0.0, cx=float(cx), cy=float(cy),
+               w=int(W), h=int(H)) for k in range(N)]
+    rec = NS(used=list(range(N)), intr=[NS(f=float(f), cx=float(cx), cy=float(cy), width=int(W), height=int(H),
+                                           k1=0.0, k2=0.0, k3=0.0)],
+             cam_group=np.zeros(N, np.int32), X=z["X"], C=z["C"], R=z["R"], obs_cam=z["obs_cam"],
+             obs_pt=z["obs_pt"], rms_px=float(z["rms_px"]))
+    greys = [((z[f"img{k}"].astype(np.float32) - np.float32(128)) / np.float32(64)).astype(np.float32)
+             for k in range(N)]
+    return z, rec, cams, greys
