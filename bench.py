@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 PM_HYPS = 11          # hypotheses per PatchMatch pixel-iteration (1 + 8 propagation + 2 random)
+PM_PROFILE = {"fp32": "profiles/pm_lane_kernel_1000x750_8src.md", "fp64": "profiles/pm_kernel_2000x1500_8src.md"}
 
 
 def parse():
@@ -39,6 +40,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--pm-precision", choices=["fp32", "fp64"], default="fp32",
+                    help="PatchMatch cost arithmetic: fp32 windows (float64-composed homographies) or the "
+                         "reference's float64 operation order (bit-exact)")
     ap.add_argument("--config", default="c2")
     ap.add_argument("--width", type=int, default=0, help="override the image width (smaller test runs)")
     ap.add_argument("--height", type=int, default=0)
@@ -181,6 +185,7 @@ def run_ours(a):
     pm.r, pm.step, pm.top_k, pm.iters = cfg.pm_radius, cfg.pm_step, top_k, iters
     pm.geo_w, pm.geo_tol, pm.dmin, pm.dmax = 0.5, 0.02, near, far
     pm.seed, pm.it0, pm.changed = 12345 + rank, 0, changed.data_ptr()
+    pm.precision = 1 if a.pm_precision == "fp32" else 0      # MVS_PM_FP32 / MVS_PM_FP64
     ev = {k: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for k in ("sweep", "pm")}
     acc = {"sweep": 0.0, "pm": 0.0}
     import ctypes
@@ -254,9 +259,12 @@ def run_ours(a):
                   "evals_per_s": sweep_evals / (ms_sweep / 1e3), "ms": round(ms_sweep, 3)}
     roof_pm = None
     if iters:
-        roof_pm = {"kernel": "pm_kernel", "bound": "fp64-issue", "evals_per_s": pm_evals / (ms_pm / 1e3),
+        roof_pm = {"kernel": "pm_lane_kernel" if a.pm_precision == "fp32" else "pm_kernel",
+                   "precision": a.pm_precision,
+                   "bound": "fp32-issue" if a.pm_precision == "fp32" else "fp64-issue",
+                   "evals_per_s": pm_evals / (ms_pm / 1e3),
                    "ms": round(ms_pm, 3), "share_of_step": round(ms_pm / (ms_pm + ms_sweep), 4),
-                   "fp64_pipe_active_ncu": 0.479, "ncu_profile": "profiles/pm_kernel_2000x1500_8src.md"}
+                   "ncu_profile": PM_PROFILE[a.pm_precision]}
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
     launches = 2 + (2 * iters if iters else 0)       # sweep + finalize + 2 colour passes per iteration
     line = {
@@ -267,6 +275,7 @@ def run_ours(a):
         "data": "synthetic seeded heightfield scene (hills + boxes, value-noise texture, nadir pinhole views)",
         "config": {"workload": f"{cfg.name}", "width": W, "height": H, "sources": nsrc, "planes": nplanes,
                    "window": 2 * r + 1, "top_k": top_k, "pm_iters": iters, "pm_window": 2 * cfg.pm_radius + 1,
+                   "pm_precision": a.pm_precision,
                    "evals_per_step": evals, "sweep_evals": sweep_evals, "pm_evals_nominal": pm_evals,
                    "l2": "inputs larger than L2 (8 sources x 48 MB)", "parallelism": f"views x{world} (replicas)"},
         "roofline": roof_sweep if dominant == "sweep" else dict(roof_sweep, note="pm dominates; see roofline_pm"),

@@ -182,13 +182,24 @@ mvs_status mvs_to_fp16(int64_t n, const float* in, void* out_half, void* stream)
 
 /* ---------------------------------------------------------------- PatchMatch */
 
+/* Arithmetic of the PatchMatch cost. */
+typedef enum mvs_pm_precision {
+    MVS_PM_FP64 = 0,     /* the reference's float64 cost, operation for operation: bit-identical
+                            results to a sequential evaluation with the same draws               */
+    MVS_PM_FP32 = 1      /* window samples and sums in float32, one float64-composed local
+                            homography per candidate and source (pinhole sources; otherwise as
+                            MVS_PM_FP64); the lanes of a pixel group evaluate its sources in
+                            parallel. Costs differ from float64 by ~1e-7, so near-ties (candidates
+                            whose costs differ by less) can be decided differently              */
+} mvs_pm_precision;
+
 typedef struct mvs_pm_args {
     int32_t H, W;
     const float* ref;                      /* (H, W) grey, NaN = masked                         */
     const float* ray;                      /* (3, H, W) world rays                              */
     const double* Cr;                      /* HOST (3) reference camera centre                  */
     int32_t S;                             /* sources, 1 .. MVS_MAX_SOURCES (else no-op, 0)     */
-    int32_t pad_;
+    int32_t precision;                     /* mvs_pm_precision (0 = MVS_PM_FP64)                */
     const float* src[MVS_MAX_SOURCES];     /* (src_h, src_w) float32 images                     */
     const float* src_depth[MVS_MAX_SOURCES]; /* same shapes or NULL (no geometric term)         */
     int32_t src_h[MVS_MAX_SOURCES];

@@ -45,7 +45,7 @@ class SweepArgs(C.Structure):
 
 
 class PMArgs(C.Structure):
-    _fields_ = [("H", i32), ("W", i32), ("ref", vp), ("ray", vp), ("Cr", vp), ("S", i32), ("pad_", i32),
+    _fields_ = [("H", i32), ("W", i32), ("ref", vp), ("ray", vp), ("Cr", vp), ("S", i32), ("precision", i32),
                 ("src", vp * MAX_SOURCES), ("src_depth", vp * MAX_SOURCES), ("src_h", i32 * MAX_SOURCES),
                 ("src_w", i32 * MAX_SOURCES), ("par", vp), ("depth", vp), ("normal", vp), ("score", vp),
                 ("active", vp), ("r", i32), ("step", i32), ("top_k", i32), ("iters", i32),

@@ -33,6 +33,7 @@ struct PMParams {
     int iw[MVS_MAX_SOURCES], ih[MVS_MAX_SOURCES];
     int pinhole[MVS_MAX_SOURCES];       // k1 = k2 = k3 = 0
     double par[MVS_MAX_SOURCES * 18];
+    double bsrc[MVS_MAX_SOURCES * 3];   // R_s (C_ref - C_s)
 };
 
 __host__ __device__ inline unsigned long long mix64(unsigned long long x) {
@@ -90,6 +91,34 @@ __device__ __forceinline__ double pm_bil(const float* im, int w, int h, double u
 #ifndef PM_SRC_PASS
 #define PM_SRC_PASS 2
 #endif
+
+// Geometric term of _pm_cost (_dense.pyx:532-555): mean over the sources with depth maps of
+// min(1, |z - d_j| / d_j / geo_tol) at the rounded projection of the window centre.
+__device__ __forceinline__ double pm_geo(const PMParams& c, double d, double rpx, double rpy, double rpz) {
+    double geo = 0.0;
+    if (c.geo_w > 0.0) {
+        const double X = c.cr0 + d * rpx, Y = c.cr1 + d * rpy, Z = c.cr2 + d * rpz;
+        int ng = 0;
+        for (int s = 0; s < c.S; ++s) {
+            if (c.dep[s] == nullptr) continue;
+            ++ng;
+            double e = 1.0, u, v, z;
+            if (pm_proj(c.par + 18 * s, X, Y, Z, u, v, z)) {
+                const int ui = (int)(u + 0.5), vv = (int)(v + 0.5);
+                if (ui >= 0 && vv >= 0 && ui < c.iw[s] && vv < c.ih[s]) {
+                    const double dj = __ldg(c.dep[s] + (long long)vv * c.iw[s] + ui);
+                    if (isfinite(dj) && dj > 0.0) {
+                        e = fabs(z - dj) / dj / c.geo_tol;
+                        if (e > 1.0) e = 1.0;
+                    }
+                }
+            }
+            geo = geo + e;
+        }
+        if (ng) geo = geo / (double)ng;
+    }
+    return geo;
+}
 
 __device__ double pm_cost(const PMParams& c, int y, int x, double d, const double* n, double& ncc_out) {
     const int H = c.H, W = c.W;
@@ -203,29 +232,7 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
     for (int a = 0; a < kk; ++a) photo = photo + ncc[a];
     photo = photo / (double)kk;
     ncc_out = photo;
-    double geo = 0.0;
-    if (c.geo_w > 0.0) {
-        const double X = c.cr0 + d * rpx, Y = c.cr1 + d * rpy, Z = c.cr2 + d * rpz;
-        int ng = 0;
-        for (int s = 0; s < c.S; ++s) {
-            if (c.dep[s] == nullptr) continue;
-            ++ng;
-            double e = 1.0, u, v, z;
-            if (pm_proj(c.par + 18 * s, X, Y, Z, u, v, z)) {
-                const int ui = (int)(u + 0.5), vv = (int)(v + 0.5);
-                if (ui >= 0 && vv >= 0 && ui < c.iw[s] && vv < c.ih[s]) {
-                    const double dj = __ldg(c.dep[s] + (long long)vv * c.iw[s] + ui);
-                    if (isfinite(dj) && dj > 0.0) {
-                        e = fabs(z - dj) / dj / c.geo_tol;
-                        if (e > 1.0) e = 1.0;
-                    }
-                }
-            }
-            geo = geo + e;
-        }
-        if (ng) geo = geo / (double)ng;
-    }
-    return (1.0 - photo) + c.geo_w * geo;
+    return (1.0 - photo) + c.geo_w * pm_geo(c, d, rpx, rpy, rpz);
 }
 
 // 8 resident blocks of 128 threads per SM (64 registers): the float64 chains are latency-bound,
@@ -329,6 +336,467 @@ __global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_con
     if (changed && c.changed) atomicAdd(c.changed, changed);
 }
 
+// ---------------------------------------------------------------- float32 evaluation (MVS_PM_FP32)
+//
+// The same visits, candidates, draws and acceptance rule as pm_kernel, with the window costs
+// evaluated in float32 and the work of one pixel spread over a group of L lanes, one per source:
+//
+//   * geometry: for a plane (d, n) and a pinhole source s, the camera point of window sample q is
+//     M_s ray_q / (n . ray_q) with M_s = b_s n^T + d (n . ray_p) R_s and b_s = R_s (C_ref - C_s)
+//     (the reference's ray-plane intersection followed by _proj, multiplied through by
+//     n . ray_q). Per (candidate, source) M_s is composed in float64, folded with f, cx, cy and an
+//     integer source anchor (U0, V0) at the window centre, and rounded once; per sample only
+//     ray_q - ray_p enters, in float32, so source positions carry ~1e-6 px of rounding error;
+//   * validity: when the four corners of the (clipped) window map inside the source with a 1 px
+//     margin and in front of it, every sample does (a projective map keeps the window inside the
+//     convex hull of its corner images) and the per-sample tests are skipped; otherwise each
+//     sample is tested as in the reference (camera depth > 1e-6, 0 <= u <= w - 1.001, ...);
+//   * sums: reference values are shifted by the window mean of the reference and source values
+//     by the source's value at the window centre, so the float32 variance terms do not cancel;
+//   * the lanes of a pixel sort their NCCs with a shuffle network (top-k mean) and sum the
+//     geometric term; every lane follows the same candidate sequence and decision.
+// Float32 costs differ from the float64 ones by ~1e-7 (measured 99.9th percentile 2e-6), so the
+// strict '<' can decide near-ties differently; the float64 mode is the bit-exact reference.
+
+#ifndef PM_LANE_MIN_BLOCKS
+#define PM_LANE_MIN_BLOCKS 3
+#endif
+
+__device__ __forceinline__ int pmf_floor(float x, float& f) {   // |x| < 2^22
+    const float t = __fadd_rd(x, 12582912.0f);
+    f = __fsub_rn(t, 12582912.0f);
+    return __float_as_int(t) - 0x4B400000;
+}
+
+// Window statistics shared by the lanes of a pixel group, fixed for one visit.
+struct PMWin {
+    const float4* w;      // NW samples (ray_q - ray_p, I - mI; I = NaN: no sample), then 4 corners
+    int nw;               // samples in the window
+    float nfin;           // samples with a finite reference value inside the image
+    float si, sii;        // sum of (I - mI) and (I - mI)^2 over those samples
+    bool allfin;          // every sample has a finite reference value inside the image
+};
+
+// One source's window sums. CHECKED: every sample tested as in the reference (camera depth,
+// source bounds, finite value) and the reference sums formed per source; otherwise (the whole
+// window maps inside the source, no sample near a test) only the three source sums are formed.
+// ALLFIN: no reference sample is missing (no masking of the reference terms).
+template <int NSIDE, bool CHECKED, bool ALLFIN>
+__device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const float* A, const float* B,
+                                               const float* C, float a0, float b0, float c0, float n0, float n1,
+                                               float n2, float denp, float lou, float hiu, float lov, float hiv,
+                                               int ub, int vb, const float* im, int sw, int last, float mJ,
+                                               float& T1, float& T2, float& X, float& S1, float& S2, float& cnt,
+                                               float& ns) {
+    // rows rolled, the samples of a row unrolled when the side is known (the checked form, rare,
+    // stays rolled to keep the instruction footprint small)
+    const int side = NSIDE > 0 ? NSIDE : 1;
+    const int NW = NSIDE > 0 ? NSIDE * NSIDE : nw;
+#pragma unroll 1
+    for (int e0 = 0; e0 < NW; e0 += side)
+#pragma unroll((NSIDE > 0 && !CHECKED) ? NSIDE : 1)
+    for (int e = e0; e < e0 + side; ++e) {
+        const float4 w = win[e];
+        const float cq = fmaf(C[0], w.x, fmaf(C[1], w.y, fmaf(C[2], w.z, c0)));
+        const float aq = fmaf(A[0], w.x, fmaf(A[1], w.y, fmaf(A[2], w.z, a0)));
+        const float bq = fmaf(B[0], w.x, fmaf(B[1], w.y, fmaf(B[2], w.z, b0)));
+        const float rc = __fdividef(1.0f, cq);
+        float ul = aq * rc, vl = bq * rc;
+        bool ok = ALLFIN || w.w == w.w;
+        if (CHECKED) {
+            const float den = fmaf(n0, w.x, fmaf(n1, w.y, fmaf(n2, w.z, denp)));
+            ok = ok && den < -1e-9f;                    // the reference skips den >= -1e-9
+            ns += ok ? 1.f : 0.f;
+            ok = ok && cq * __fdividef(1.0f, den) > 1e-6f && ul >= lou && ul <= hiu && vl >= lov && vl <= hiv;
+            ul = ok ? ul : 0.f;
+            vl = ok ? vl : 0.f;
+        }
+        float fu, fv;
+        const int xi = pmf_floor(ul, fu) + ub + 0x4B400000;
+        const int yi = pmf_floor(vl, fv) + vb + 0x4B400000;
+        // the clamp keeps every tap inside the image whatever the inputs
+        const int o = min(max(yi * sw + xi, 0), last);
+        const float fx = ul - fu, fy = vl - fv;
+        const float* t = im + o;
+        const float t00 = __ldg(t), t01 = __ldg(t + 1), t10 = __ldg(t + sw), t11 = __ldg(t + sw + 1);
+        const float top = fmaf(fx, t01 - t00, t00), bot = fmaf(fx, t11 - t10, t10);
+        const float J = fmaf(fy, bot - top, top);
+        if (CHECKED) ok = ok && fabsf(J) <= 3.4e38f;
+        float Jp = J - mJ, Iv = w.w;
+        if (CHECKED || !ALLFIN) {
+            Jp = ok ? Jp : 0.f;
+            Iv = ok ? Iv : 0.f;
+        }
+        T1 += Jp;
+        T2 = fmaf(Jp, Jp, T2);
+        X = fmaf(Iv, Jp, X);
+        if (CHECKED) {
+            S1 += Iv;
+            S2 = fmaf(Iv, Iv, S2);
+            cnt += ok ? 1.f : 0.f;
+        }
+    }
+}
+
+// float32 photo term (top-k mean NCC) of plane (d, n) at pixel (y, x); n . ray_p = ndr < -1e-6.
+// Called by all L lanes of a pixel group (lane s evaluates source s); returns the same value in
+// every lane.
+template <int L, int NSIDE>
+__device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
+                               const double* n, double ndr, int s, unsigned gmask) {
+    const double num = d * ndr;
+    const float n0 = (float)n[0], n1 = (float)n[1], n2 = (float)n[2], denp = (float)ndr;
+    const bool has = s < c.S;
+    const int sl = has ? s : 0;
+    const int NW = NSIDE > 0 ? NSIDE * NSIDE : wn.nw;
+    const float4* win = wn.w;
+    // ---- per (candidate, source) local map. The camera point of sample q is M ray_q / (n.ray_q),
+    // M = b n^T + num R. The window centre is formed in float64 (b (n.ray_p) + num R ray_p), the
+    // rows of M (which only multiply ray_q - ray_p) in float32.
+    const double* p = c.par + 18 * sl;
+    const double* bs = c.bsrc + 3 * sl;
+    const double rp[3] = {rpx, rpy, rpz};
+    double cen[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double Rr = fma(p[3 * i], rp[0], fma(p[3 * i + 1], rp[1], p[3 * i + 2] * rp[2]));
+        cen[i] = fma(bs[i], ndr, num * Rr);
+    }
+    const double xp = cen[0], yp = cen[1], zp = cen[2];
+    const double f = p[12], pcx = p[16], pcy = p[17];
+    // the centre's camera depth is zp / ndr: in front of the source needs zp < 0
+    const bool front = zp < 0.0;
+    const float ff = (float)f, rzf = front ? __fdividef(1.0f, (float)zp) : 0.f;
+    const float ucf = fmaf(ff, (float)xp * rzf, (float)pcx), vcf = fmaf(ff, (float)yp * rzf, (float)pcy);
+    const float Uf = fminf(fmaxf(floorf(ucf), -1048576.f), 1048576.f);
+    const float Vf = fminf(fmaxf(floorf(vcf), -1048576.f), 1048576.f);
+    const bool anchor = front && Uf == Uf && Vf == Vf;
+    const double U0d = anchor ? (double)Uf : 0.0, V0d = anchor ? (double)Vf : 0.0;
+    const double au = pcx - U0d, av = pcy - V0d;
+    const float a0 = (float)fma(f, xp, au * zp), b0 = (float)fma(f, yp, av * zp), c0 = (float)zp;
+    const float auf = (float)au, avf = (float)av, numf = (float)num;
+    float A[3], B[3], C[3];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        const float nj = j == 0 ? n0 : (j == 1 ? n1 : n2);
+        const float mx = fmaf((float)bs[0], nj, numf * (float)p[j]);
+        const float my = fmaf((float)bs[1], nj, numf * (float)p[3 + j]);
+        const float mz = fmaf((float)bs[2], nj, numf * (float)p[6 + j]);
+        A[j] = fmaf(ff, mx, auf * mz);
+        B[j] = fmaf(ff, my, avf * mz);
+        C[j] = mz;
+    }
+    const int sw = c.iw[sl], sh = c.ih[sl];
+    const float lou = (float)(-U0d), lov = (float)(-V0d);
+    const float hiu = (float)(((double)sw - 1.001) - U0d), hiv = (float)(((double)sh - 1.001) - V0d);
+    const float* im = c.img[sl];
+    // integer tap position = floor bits + (U0 - magic): one add per coordinate
+    const int ub = (int)U0d - 0x4B400000, vb = (int)V0d - 0x4B400000;
+    const int last = sh * sw - sw - 2;                    // largest valid top-left tap offset
+    // ---- corners: the whole window in front and inside (outside) the source
+    bool den_ok = true, inside = anchor, front_all = true;
+    int out_lo_u = 0, out_hi_u = 0, out_lo_v = 0, out_hi_v = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float4 w = win[NW + k];
+        const float den = fmaf(n0, w.x, fmaf(n1, w.y, fmaf(n2, w.z, denp)));
+        const float cq = fmaf(C[0], w.x, fmaf(C[1], w.y, fmaf(C[2], w.z, c0)));
+        const float aq = fmaf(A[0], w.x, fmaf(A[1], w.y, fmaf(A[2], w.z, a0)));
+        const float bq = fmaf(B[0], w.x, fmaf(B[1], w.y, fmaf(B[2], w.z, b0)));
+        const float rc = __fdividef(1.0f, cq);
+        const float ul = aq * rc, vl = bq * rc;
+        den_ok = den_ok && den < -1e-3f;
+        front_all = front_all && cq < 1e-2f * den;
+        inside = inside && ul >= lou + 1.f && ul <= hiu - 1.f && vl >= lov + 1.f && vl <= hiv - 1.f;
+        out_lo_u += ul < lou - 1.f;
+        out_hi_u += ul > hiu + 1.f;
+        out_lo_v += vl < lov - 1.f;
+        out_hi_v += vl > hiv + 1.f;
+    }
+    inside = inside && den_ok && front_all;
+    const bool outside = den_ok && front_all && anchor &&
+                         (out_lo_u == 4 || out_hi_u == 4 || out_lo_v == 4 || out_hi_v == 4);
+    // ---- source shift: the source at the window centre (the anchor), else 0
+    float mJ = 0.f;
+    if (anchor && !outside) {
+        const float ul = a0 / c0, vl = b0 / c0;
+        if (ul >= lou && ul <= hiu && vl >= lov && vl <= hiv) {
+            float fu, fv;
+            const int xi = pmf_floor(ul, fu) + ub + 0x4B400000, yi = pmf_floor(vl, fv) + vb + 0x4B400000;
+            const int o = min(max(yi * sw + xi, 0), last);
+            const float fx = ul - fu, fy = vl - fv;
+            const float t00 = __ldg(im + o), t01 = __ldg(im + o + 1), t10 = __ldg(im + o + sw), t11 = __ldg(im + o + sw + 1);
+            const float top = fmaf(fx, t01 - t00, t00), bot = fmaf(fx, t11 - t10, t10);
+            const float J = fmaf(fy, bot - top, top);
+            if (fabsf(J) <= 3.4e38f) mJ = J;
+        }
+    }
+    // ---- window sums
+    float T1 = 0.f, T2 = 0.f, X = 0.f, S1 = 0.f, S2 = 0.f, cnt = 0.f, ns = 0.f;
+    bool checked = !den_ok;                   // the count of samples needs the per-sample test
+    if (has && !outside && inside) {
+        if (wn.allfin) {
+            pm_window_sums<NSIDE, false, true>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+                                               ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+        } else {
+            pm_window_sums<NSIDE, false, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+                                                ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+        }
+        // a non-finite source value in the window poisons the sums: redo the source checked
+        if (fabsf(T2) <= 3.4e38f && fabsf(X) <= 3.4e38f) {
+            S1 = wn.si; S2 = wn.sii; cnt = wn.nfin;
+        } else {
+            checked = true;
+        }
+    } else if (has && !outside) {
+        checked = true;
+    }
+    if (checked) {
+        T1 = T2 = X = S1 = S2 = cnt = ns = 0.f;
+        pm_window_sums<NSIDE, true, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+                                           ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+    }
+    // samples counted by the reference (finite reference value, n.ray_q < -1e-9): with every
+    // corner's n.ray_q < -1e-3 that is every finite sample; otherwise each lane counted them
+    if (den_ok) ns = wn.nfin;
+    // ---- NCC of this lane's source (_pm_cost: -1 below the count gate, 0 below the variance floor)
+    float ncc = -INFINITY;                                 // idle lanes sort last
+    if (has) {
+        if (ns < 4.f || (double)cnt < 0.7 * (double)ns) {
+            ncc = -1.f;
+        } else {
+            const float rc = 1.0f / cnt;
+            const float mi = S1 * rc, mj = T1 * rc;
+            const float vi = fmaf(-mi, mi, S2 * rc), vj = fmaf(-mj, mj, T2 * rc);
+            const float cv = fmaf(-mi, mj, X * rc);
+            ncc = (vi < 1e-8f || vj < 1e-8f) ? 0.f : cv * rsqrtf(vi * vj);
+            if (!(fabsf(ncc) <= 3.4e38f)) ncc = 0.f;
+        }
+    }
+    // ---- descending bitonic sort over the group, then the mean of the first top_k
+    const int lane = threadIdx.x & (L - 1);
+#pragma unroll
+    for (int k = 2; k <= L; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const float o = __shfl_xor_sync(gmask, ncc, j, L);
+            const bool keep_max = ((lane & k) == 0) == ((lane & j) == 0);
+            ncc = keep_max ? fmaxf(ncc, o) : fminf(ncc, o);
+        }
+    }
+    const int kk = c.top_k < c.S ? c.top_k : c.S;
+    float sum = lane < kk ? ncc : 0.f;
+#pragma unroll
+    for (int o = L >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, L);
+    return sum / (float)kk;
+}
+
+// Geometric term over the group: lane s contributes source s's error (float64, as pm_geo).
+template <int L>
+__device__ __forceinline__ double pm_geo_lane(const PMParams& c, double d, double rpx, double rpy, double rpz, int s,
+                                              unsigned gmask, int ng) {
+    double e = 0.0;
+    if (s < c.S && c.dep[s] != nullptr) {
+        const double X = c.cr0 + d * rpx, Y = c.cr1 + d * rpy, Z = c.cr2 + d * rpz;
+        double u, v, z;
+        e = 1.0;
+        if (pm_proj(c.par + 18 * s, X, Y, Z, u, v, z)) {
+            const int ui = (int)(u + 0.5), vv = (int)(v + 0.5);
+            if (ui >= 0 && vv >= 0 && ui < c.iw[s] && vv < c.ih[s]) {
+                const double dj = __ldg(c.dep[s] + (long long)vv * c.iw[s] + ui);
+                if (isfinite(dj) && dj > 0.0) {
+                    e = fabs(z - dj) / dj / c.geo_tol;
+                    if (e > 1.0) e = 1.0;
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int o = L >> 1; o > 0; o >>= 1) e += __shfl_xor_sync(gmask, e, o, L);
+    return e / (double)ng;
+}
+
+// Samples along one side of the window: offsets -r, -r + step, ... <= r.
+__host__ __device__ inline int pm_side(int r, int step) { return (2 * r) / step + 1; }
+
+template <int L, int NSIDE>
+__global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const __grid_constant__ PMParams c) {
+    extern __shared__ float4 pm_win[];
+    const int H = c.H, W = c.W;
+    const int half_w = (W + 1) / 2;
+    const int lane = threadIdx.x & (L - 1);
+    const unsigned gmask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (threadIdx.x & 31 & ~(L - 1));
+    const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / L;
+    const int y = (int)(t / half_w);
+    if (y >= H) return;
+    const int x = 2 * (int)(t - (long long)y * half_w) + ((y + c.colour) & 1);
+    if (x >= W) return;
+    const long long HW = (long long)H * W, idx = (long long)y * W + x;
+    if (!c.active[idx]) return;
+    int ng = 0;
+    for (int s = 0; s < c.S; ++s) ng += c.dep[s] != nullptr;
+    const bool use_geo = c.geo_w > 0.0 && ng > 0;
+    // ---- stage the window once per visit: ray offsets and reference values (NaN = no sample),
+    // then the four corners of the clipped window; the window mean of the reference is the
+    // shift of the float32 sums
+    const int side = NSIDE > 0 ? NSIDE : pm_side(c.r, c.step);
+    const int nw = side * side;
+    float4* win = pm_win + (threadIdx.x / L) * (nw + 4);
+    const float rpx = __ldg(c.ray + idx), rpy = __ldg(c.ray + HW + idx), rpz = __ldg(c.ray + 2 * HW + idx);
+    PMWin wn;
+    wn.w = win;
+    wn.nw = nw;
+    {
+        float sum = 0.f, k = 0.f;
+        for (int e = lane; e < nw + 4; e += L) {
+            int yy, xx;
+            if (e < nw) {
+                yy = y - c.r + (e / side) * c.step;
+                xx = x - c.r + (e % side) * c.step;
+            } else {
+                const int k4 = e - nw;
+                yy = k4 < 2 ? max(y - c.r, 0) : min(y + c.r, H - 1);
+                xx = (k4 & 1) ? min(x + c.r, W - 1) : max(x - c.r, 0);
+            }
+            float4 v = make_float4(0.f, 0.f, 0.f, __int_as_float(0x7fc00000));
+            if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
+                const long long q = (long long)yy * W + xx;
+                v.x = __ldg(c.ray + q) - rpx;
+                v.y = __ldg(c.ray + HW + q) - rpy;
+                v.z = __ldg(c.ray + 2 * HW + q) - rpz;
+                const float I = __ldg(c.ref + q);
+                if (e < nw && fabsf(I) <= 3.4e38f) {
+                    v.w = I;
+                    sum += I;
+                    k += 1.f;
+                }
+            }
+            win[e] = v;
+        }
+#pragma unroll
+        for (int o = L >> 1; o > 0; o >>= 1) {
+            sum += __shfl_xor_sync(gmask, sum, o, L);
+            k += __shfl_xor_sync(gmask, k, o, L);
+        }
+        // shift of the float32 sums: the window mean of the reference
+        const float mI = k > 0.f ? sum / k : 0.f;
+        float si = 0.f, sii = 0.f;
+        for (int e = lane; e < nw; e += L) {
+            const float I = win[e].w;
+            if (I == I) {
+                const float Ip = I - mI;
+                win[e].w = Ip;
+                si += Ip;
+                sii = fmaf(Ip, Ip, sii);
+            }
+        }
+#pragma unroll
+        for (int o = L >> 1; o > 0; o >>= 1) {
+            si += __shfl_xor_sync(gmask, si, o, L);
+            sii += __shfl_xor_sync(gmask, sii, o, L);
+        }
+        wn.nfin = k;
+        wn.si = si;
+        wn.sii = sii;
+        wn.allfin = k == (float)nw;
+        __syncwarp(gmask);
+    }
+    const double rx = rpx, ry = rpy, rz = rpz;
+    // cost of a candidate: _pm_cost's 10 for an invalid plane, else (1 - photo) + geo_w * geo
+    auto cost = [&](double d, const double* nb, double& photo) -> double {
+        const double ndr = nb[0] * rx + nb[1] * ry + nb[2] * rz;
+        if (ndr >= -1e-6 || d <= 0.0) {
+            photo = 0.0;
+            return 10.0;
+        }
+        photo = (double)pm_photo_lane<L, NSIDE>(c, wn, rpx, rpy, rpz, d, nb, ndr, lane, gmask);
+        const double geo = use_geo ? pm_geo_lane<L>(c, d, rx, ry, rz, lane, gmask, ng) : 0.0;
+        return (1.0 - photo) + c.geo_w * geo;
+    };
+    const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
+    const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
+    float dcur = c.depth[idx];
+    float ncur[3] = {c.normal[idx], c.normal[HW + idx], c.normal[2 * HW + idx]};
+    double best, sc, ph;
+    unsigned long long changed = 0;
+    const double cached = c.cost_cache ? c.cost_cache[idx] : __longlong_as_double(0x7ff8000000000000LL);
+    if (isfinite(dcur) && cached == cached) {
+        best = cached;
+        sc = c.score_cache[idx];
+    } else if (isfinite(dcur)) {
+        const double n[3] = {ncur[0], ncur[1], ncur[2]};
+        best = cost((double)dcur, n, ph);
+        sc = ph;
+    } else {
+        best = 1e9;
+        sc = -1.0;
+    }
+    for (int k = 0; k < 8; ++k) {
+        const int yn = y + offy[k], xn = x + offx[k];
+        if (yn < 0 || xn < 0 || yn >= H || xn >= W) continue;
+        const long long nidx = (long long)yn * W + xn;
+        const float dnb = c.depth[nidx];
+        if (!isfinite(dnb)) continue;
+        const double nb[3] = {c.normal[nidx], c.normal[HW + nidx], c.normal[2 * HW + nidx]};
+        const double dn = nb[0] * __ldg(c.ray + nidx) + nb[1] * __ldg(c.ray + HW + nidx) + nb[2] * __ldg(c.ray + 2 * HW + nidx);
+        const double ndr = nb[0] * rx + nb[1] * ry + nb[2] * rz;
+        if (ndr >= -1e-6) continue;
+        const double dp = (double)dnb * dn / ndr;
+        if (dp < c.dmin || dp > c.dmax) continue;
+        const double cst = cost(dp, nb, ph);
+        if (cst < best) {
+            best = cst;
+            sc = ph;
+            dcur = (float)dp;
+            ncur[0] = (float)nb[0]; ncur[1] = (float)nb[1]; ncur[2] = (float)nb[2];
+            ++changed;
+        }
+    }
+    if (isfinite(dcur)) {
+        // the 8 draws of the two trials: lane k computes draw k (mod L), the group shares them
+        double mine[8 / L > 0 ? 8 / L : 1];
+#pragma unroll
+        for (int r0 = 0; r0 < 8; r0 += L) mine[r0 / L] = r0 + lane < 8 ? pm_uniform(c.seed, c.it, idx, r0 + lane) : 0.0;
+        auto draw = [&](int k) { return __shfl_sync(gmask, mine[k / L], k % L, L); };
+        for (int tr = 0; tr < 2; ++tr) {
+            const double u0 = draw(4 * tr + 0);
+            const double u1 = draw(4 * tr + 1);
+            const double u2 = draw(4 * tr + 2);
+            const double u3 = draw(4 * tr + 3);
+            const double dp = (double)dcur * (1.0 + c.dd_scale * (2.0 * u0 - 1.0));
+            double nb[3];
+            nb[0] = (double)ncur[0] + c.nn_scale * (2.0 * u1 - 1.0);
+            nb[1] = (double)ncur[1] + c.nn_scale * (2.0 * u2 - 1.0);
+            nb[2] = (double)ncur[2] + c.nn_scale * (2.0 * u3 - 1.0);
+            const double nn = sqrt(nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]);
+            if (nn < 1e-9 || dp < c.dmin || dp > c.dmax) continue;
+            nb[0] = nb[0] / nn;
+            nb[1] = nb[1] / nn;
+            nb[2] = nb[2] / nn;
+            const double cst = cost(dp, nb, ph);
+            if (cst < best) {
+                best = cst;
+                sc = ph;
+                dcur = (float)dp;
+                ncur[0] = (float)nb[0]; ncur[1] = (float)nb[1]; ncur[2] = (float)nb[2];
+                ++changed;
+            }
+        }
+    }
+    if (lane != 0) return;
+    if (c.cost_cache) {
+        const bool keep = changed == 0 && isfinite(dcur);
+        c.cost_cache[idx] = keep ? best : __longlong_as_double(0x7ff8000000000000LL);
+        if (keep) c.score_cache[idx] = sc;
+    }
+    c.depth[idx] = dcur;
+    c.normal[idx] = ncur[0];
+    c.normal[HW + idx] = ncur[1];
+    c.normal[2 * HW + idx] = ncur[2];
+    c.score[idx] = (float)sc;
+    if (changed && c.changed) atomicAdd(c.changed, changed);
+}
+
 }  // namespace mvs
 
 using namespace mvs;
@@ -369,6 +837,19 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     }
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
     const long long HW = (long long)a->H * a->W;
+    if (a->precision != MVS_PM_FP64 && a->precision != MVS_PM_FP32)
+        return fail(MVS_ERR_VALUE, "pm_refine: unknown precision %d", a->precision);
+    // float32 evaluation needs pinhole sources (the local map is a homography)
+    bool fast = a->precision == MVS_PM_FP32;
+    for (int s = 0; s < a->S && fast; ++s) fast = p.pinhole[s] != 0;
+    if (fast) {
+        for (int s = 0; s < a->S; ++s) {
+            const double* q = a->par + 18 * s;
+            // b_s = R_s (C_ref - C_s)
+            const double e0 = a->Cr[0] - q[9], e1 = a->Cr[1] - q[10], e2 = a->Cr[2] - q[11];
+            for (int i = 0; i < 3; ++i) p.bsrc[3 * s + i] = q[3 * i] * e0 + q[3 * i + 1] * e1 + q[3 * i + 2] * e2;
+        }
+    }
     void* cache = nullptr;
     if (a->iters > 1) {   // the cache pays off from the second iteration on
         if (cudaMallocAsync(&cache, (size_t)HW * 2 * sizeof(double), st) == cudaSuccess) {
@@ -380,7 +861,25 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         }
     }
     const long long nthreads = (long long)a->H * ((a->W + 1) / 2);
-    const unsigned grid = (unsigned)((nthreads + 127) / 128);
+    // float32 lanes: one per source; a block holds as many pixel groups as its staged windows fit
+    const int lanes = a->S <= 4 ? 4 : (a->S <= 8 ? 8 : 16);
+    const int side = pm_side(a->r, a->step);
+    const size_t win_bytes = (size_t)(side * side + 4) * sizeof(float4);
+    int groups = 256 / lanes;
+    while (groups > 1 && (size_t)groups * win_bytes > 96 * 1024) groups >>= 1;
+    const int block = fast ? groups * lanes : 128;
+    const size_t smem = fast ? (size_t)groups * win_bytes : 0;
+    void (*lane_kernel)(PMParams) = nullptr;
+    if (fast) {
+#define PM_PICK(LN)                                                              \
+    lane_kernel = side == 7 ? pm_lane_kernel<LN, 7> : side == 5 ? pm_lane_kernel<LN, 5> \
+                                                    : pm_lane_kernel<LN, 0>;
+        if (lanes == 4) { PM_PICK(4) } else if (lanes == 8) { PM_PICK(8) } else { PM_PICK(16) }
+#undef PM_PICK
+        MVS_CUDA(cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                 "pm_refine: shared-memory carve-out");
+    }
+    const unsigned grid = fast ? (unsigned)((nthreads * lanes + block - 1) / block) : (unsigned)((nthreads + 127) / 128);
     for (int it = 0; it < a->iters; ++it) {
         const int git = a->it0 + it;
         p.it = git;
@@ -388,7 +887,11 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         p.nn_scale = 0.3 / (double)(git + 1);
         for (int colour = 0; colour < 2; ++colour) {
             p.colour = colour;
-            pm_kernel<<<grid, 128, 0, st>>>(p);
+            if (!fast) {
+                pm_kernel<<<grid, 128, 0, st>>>(p);
+            } else {
+                lane_kernel<<<grid, block, smem, st>>>(p);
+            }
             mvs_status ks = check_launch("pm_refine kernel");
             if (ks != MVS_OK) {
                 if (cache) cudaFreeAsync(cache, st);

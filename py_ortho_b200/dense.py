@@ -224,12 +224,21 @@ def C_addr(struct) -> int:
 
 
 # ------------------------------------------------------------------ pm_refine
+PM_PRECISIONS = {"fp64": 0, "fp32": 1}     # mvs_pm_precision
+
 def pm_refine(ref, ray, Cr, srcs: Sequence, src_depths: Sequence, par, depth, normal, score, active, r: int,
               step: int, top_k: int, geo_w: float, geo_tol: float, iters: int, dmin: float, dmax: float,
-              seed: int, it0: int = 0) -> int:
+              seed: int, it0: int = 0, precision: str = "fp64") -> int:
     """Slanted-plane PatchMatch repair (reference: _dense.pyx:566-666); depth / normal / score are
     updated in place; returns the number of accepted hypothesis changes. Random trials use
-    counter-based draws (mvs_pm_uniform) instead of one sequential xorshift stream."""
+    counter-based draws (mvs_pm_uniform) instead of one sequential xorshift stream.
+
+    precision: "fp64" evaluates the reference's float64 cost operation for operation (bit-identical
+    to a sequential evaluation with the same draws); "fp32" evaluates the windows in float32 from
+    one float64-composed homography per candidate and source (costs within ~1e-6 of float64;
+    near-ties may be decided differently)."""
+    if precision not in PM_PRECISIONS:
+        raise ValueError(f"pm_refine: precision must be one of {sorted(PM_PRECISIONS)}")
     S = len(srcs)
     if S == 0 or S > L.MAX_SOURCES:
         return 0
@@ -259,6 +268,7 @@ def pm_refine(ref, ray, Cr, srcs: Sequence, src_depths: Sequence, par, depth, no
         changed = torch.zeros(1, dtype=torch.int64, device=ref_t.device)
         a = L.PMArgs()
         a.H, a.W, a.S = H, W, S
+        a.precision = PM_PRECISIONS[precision]
         a.ref, a.ray, a.Cr = ref_t.data_ptr(), ray_t.data_ptr(), L.host_ptr(cr_h)
         for k in range(S):
             a.src[k] = src_t[k].data_ptr()

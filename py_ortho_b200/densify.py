@@ -44,6 +44,7 @@ class DepthOptions:
     cache_mb: int = 1200
     workers: int = 0
     precision: int = L.PREC_FP32      # FP16 storage of source images (constant-plane sweeps only)
+    pm_precision: str = "fp64"        # PatchMatch cost: "fp64" (the reference's arithmetic) or "fp32"
 
 
 class _Cam:

@@ -45,6 +45,7 @@ class DepthRequest:
     pm_step: int = 1
     depth_range: tuple = (1e-3, 1e9)
     seed: int = 0
+    pm_precision: str = "fp32"       # PatchMatch cost arithmetic (mvs_pm_precision)
     arrival: float = 0.0             # seconds from the start of the trace
     rid: int = 0
 
@@ -293,6 +294,7 @@ def pm_args(ref, ray, ref_cam, srcs, src_cams, depth, normal, score, active, req
     a.r, a.step, a.top_k, a.iters = req.pm_radius, req.pm_step, req.top_k, iters
     a.geo_w, a.geo_tol, a.dmin, a.dmax = 0.0, 0.02, float(req.depth_range[0]), float(req.depth_range[1])
     a.seed, a.it0, a.changed = req.seed, 0, 0
+    a.precision = 1 if req.pm_precision == "fp32" else 0
     return a, (par, Cr)
 
 

@@ -177,7 +177,7 @@ def repair(k: int, raw: Dict[int, torch.Tensor], score: torch.Tensor, low: torch
             changed = dense.pm_refine(ref, ray, np.asarray(cr.C, np.float64), srcs, [raw[j] for j in js], par, D,
                                       normal, S, active, opt.pm_window, opt.pm_step, opt.top_k, opt.pm_geo_weight,
                                       float(np.median(list(tol.values()))), opt.pm_iters, rng[0], rng[1],
-                                      k * 2654435761 % 2**32)
+                                      k * 2654435761 % 2**32, precision=getattr(opt, "pm_precision", "fp64"))
     D = torch.where((S < opt.min_ncc) | low, torch.full_like(D, float("nan")), D)
     return D, changed, n_active
 
