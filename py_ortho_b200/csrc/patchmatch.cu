@@ -438,16 +438,14 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
     }
 }
 
-// float32 photo term (top-k mean NCC) of plane (d, n) at pixel (y, x); n . ray_p = ndr < -1e-6.
-// Called by all L lanes of a pixel group (lane s evaluates source s); returns the same value in
-// every lane.
-template <int L, int NSIDE>
-__device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
-                               const double* n, double ndr, int s, unsigned gmask) {
+// float32 NCC of one (candidate, source) unit: plane (d, n) at the window's pixel, source s
+// (s < S); n . ray_p = ndr < -1e-6. Follows _pm_cost: -1 below the count gate, 0 below the
+// variance floor.
+template <int NSIDE>
+__device__ float pm_unit_ncc(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
+                             const double* n, double ndr, int sl) {
     const double num = d * ndr;
     const float n0 = (float)n[0], n1 = (float)n[1], n2 = (float)n[2], denp = (float)ndr;
-    const bool has = s < c.S;
-    const int sl = has ? s : 0;
     const int NW = NSIDE > 0 ? NSIDE * NSIDE : wn.nw;
     const float4* win = wn.w;
     // ---- per (candidate, source) local map. The camera point of sample q is M ray_q / (n.ray_q),
@@ -534,7 +532,7 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
     // ---- window sums
     float T1 = 0.f, T2 = 0.f, X = 0.f, S1 = 0.f, S2 = 0.f, cnt = 0.f, ns = 0.f;
     bool checked = !den_ok;                   // the count of samples needs the per-sample test
-    if (has && !outside && inside) {
+    if (!outside && inside) {
         if (wn.allfin) {
             pm_window_sums<NSIDE, false, true>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
                                                ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
@@ -548,7 +546,7 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
         } else {
             checked = true;
         }
-    } else if (has && !outside) {
+    } else if (!outside) {
         checked = true;
     }
     if (checked) {
@@ -559,9 +557,8 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
     // samples counted by the reference (finite reference value, n.ray_q < -1e-9): with every
     // corner's n.ray_q < -1e-3 that is every finite sample; otherwise each lane counted them
     if (den_ok) ns = wn.nfin;
-    // ---- NCC of this lane's source (_pm_cost: -1 below the count gate, 0 below the variance floor)
-    float ncc = -INFINITY;                                 // idle lanes sort last
-    if (has) {
+    float ncc;
+    {
         if (ns < 4.f || (double)cnt < 0.7 * (double)ns) {
             ncc = -1.f;
         } else {
@@ -573,6 +570,15 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
             if (!(fabsf(ncc) <= 3.4e38f)) ncc = 0.f;
         }
     }
+    return ncc;
+}
+
+// float32 photo term (top-k mean NCC) of plane (d, n): the L lanes of a pixel group evaluate one
+// source each and sort their NCCs with a shuffle network; every lane returns the same value.
+template <int L, int NSIDE>
+__device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
+                               const double* n, double ndr, int s, unsigned gmask) {
+    float ncc = s < c.S ? pm_unit_ncc<NSIDE>(c, wn, rpx, rpy, rpz, d, n, ndr, s) : -INFINITY;   // idle lanes sort last
     // ---- descending bitonic sort over the group, then the mean of the first top_k
     const int lane = threadIdx.x & (L - 1);
 #pragma unroll
@@ -589,6 +595,47 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
 #pragma unroll
     for (int o = L >> 1; o > 0; o >>= 1) sum += __shfl_xor_sync(gmask, sum, o, L);
     return sum / (float)kk;
+}
+
+// float32 photo term of plane (d, n) evaluated by one lane over all sources (the propagation
+// step gives each lane its own candidate); the top-k list is kept sorted in registers.
+template <int NSIDE, int KM>
+__device__ __forceinline__ float pm_photo_cand_k(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+                                                 double d, const double* n, double ndr) {
+    const int kk = c.top_k < c.S ? c.top_k : c.S;
+    float top[KM];
+#pragma unroll
+    for (int q = 0; q < KM; ++q) top[q] = -INFINITY;
+#pragma unroll 1
+    for (int s = 0; s < c.S; ++s) {
+        float x = pm_unit_ncc<NSIDE>(c, wn, rpx, rpy, rpz, d, n, ndr, s);
+#pragma unroll
+        for (int q = 0; q < KM; ++q) {
+            if (q < kk) {
+                const float hi = fmaxf(top[q], x), lo = fminf(top[q], x);
+                top[q] = hi;
+                x = lo;
+            }
+        }
+    }
+    float sum = 0.f;
+#pragma unroll
+    for (int q = 0; q < KM; ++q) sum += q < kk ? top[q] : 0.f;
+    return sum / (float)kk;
+}
+
+template <int NSIDE>
+__device__ __noinline__ float pm_photo_cand_wide(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+                                                 double d, const double* n, double ndr) {
+    return pm_photo_cand_k<NSIDE, MVS_MAX_SOURCES>(c, wn, rpx, rpy, rpz, d, n, ndr);
+}
+
+// top_k <= 2 (the reference's default) keeps a 2-entry list; wider lists take an out-of-line call
+template <int NSIDE>
+__device__ __forceinline__ float pm_photo_cand(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+                                               double d, const double* n, double ndr) {
+    if (c.top_k <= 2) return pm_photo_cand_k<NSIDE, 2>(c, wn, rpx, rpy, rpz, d, n, ndr);
+    return pm_photo_cand_wide<NSIDE>(c, wn, rpx, rpy, rpz, d, n, ndr);
 }
 
 // Geometric term over the group: lane s contributes source s's error (float64, as pm_geo).
@@ -731,7 +778,30 @@ __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const 
         best = 1e9;
         sc = -1.0;
     }
-    for (int k = 0; k < 8; ++k) {
+    // propagation: the neighbours' planes do not change during a colour pass, so the 8 candidate
+    // costs are independent of one another. Lane k (mod L) evaluates candidate k over all sources;
+    // then every lane takes the decisions in the reference's order from the shared results.
+    auto cost_cand = [&](double d, const double* nb, double& photo) -> double {
+        const double ndr = nb[0] * rx + nb[1] * ry + nb[2] * rz;
+        if (ndr >= -1e-6 || d <= 0.0) {
+            photo = 0.0;
+            return 10.0;
+        }
+        photo = (double)pm_photo_cand<NSIDE>(c, wn, rpx, rpy, rpz, d, nb, ndr);
+        const double geo = use_geo ? pm_geo(c, d, rx, ry, rz) : 0.0;
+        return (1.0 - photo) + c.geo_w * geo;
+    };
+    constexpr int PR = (8 + L - 1) / L;          // candidates per lane
+    double pcost[PR];
+    float pphoto[PR], pd[PR], pn[PR][3];
+    bool pok[PR];
+#pragma unroll
+    for (int r0 = 0; r0 < PR; ++r0) {
+        const int k = r0 * L + lane;
+        pok[r0] = false;
+        pcost[r0] = 0.0;
+        pphoto[r0] = pd[r0] = pn[r0][0] = pn[r0][1] = pn[r0][2] = 0.f;
+        if (k >= 8) continue;
         const int yn = y + offy[k], xn = x + offx[k];
         if (yn < 0 || xn < 0 || yn >= H || xn >= W) continue;
         const long long nidx = (long long)yn * W + xn;
@@ -743,12 +813,28 @@ __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const 
         if (ndr >= -1e-6) continue;
         const double dp = (double)dnb * dn / ndr;
         if (dp < c.dmin || dp > c.dmax) continue;
-        const double cst = cost(dp, nb, ph);
-        if (cst < best) {
+        double phc;
+        pcost[r0] = cost_cand(dp, nb, phc);
+        pphoto[r0] = (float)phc;
+        pd[r0] = (float)dp;
+        pn[r0][0] = (float)nb[0]; pn[r0][1] = (float)nb[1]; pn[r0][2] = (float)nb[2];
+        pok[r0] = true;
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int from = k % L, r0 = k / L;
+        const bool ok = __shfl_sync(gmask, (int)pok[r0], from, L) != 0;
+        const double cst = __shfl_sync(gmask, pcost[r0], from, L);
+        const float phk = __shfl_sync(gmask, pphoto[r0], from, L);
+        const float dk = __shfl_sync(gmask, pd[r0], from, L);
+        const float n0 = __shfl_sync(gmask, pn[r0][0], from, L);
+        const float n1 = __shfl_sync(gmask, pn[r0][1], from, L);
+        const float n2 = __shfl_sync(gmask, pn[r0][2], from, L);
+        if (ok && cst < best) {
             best = cst;
-            sc = ph;
-            dcur = (float)dp;
-            ncur[0] = (float)nb[0]; ncur[1] = (float)nb[1]; ncur[2] = (float)nb[2];
+            sc = phk;
+            dcur = dk;
+            ncur[0] = n0; ncur[1] = n1; ncur[2] = n2;
             ++changed;
         }
     }
