@@ -252,7 +252,7 @@ def run_ours(a):
     b_src = 2.0 if prec == L.PREC_FP16 else 4.0
     bytes_per_eval = b_src + (12.0 + 20.0) / (nplanes * nsrc)
     sweep_gbs = sweep_evals * bytes_per_eval / (ms_sweep / 1e3) / 1e9
-    traffic = read_traffic("sweep")
+    traffic = read_traffic("sweep_kernel")
     roof_sweep = {"kernel": "sweep_kernel", "bound": "hbm", "achieved": round(sweep_gbs, 1),
                   "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sweep_gbs / peaks["hbm_gbs"], 4),
                   "traffic": traffic, "peak_source": peaks["source"], "bytes_per_eval": round(bytes_per_eval, 4),
