@@ -304,6 +304,36 @@ mvs_status mvs_consistency(const mvs_consistency_args* args, void* stream);
 mvs_status mvs_init_normals(int32_t H, int32_t W, const float* depth, const float* ray, float* normal,
                             void* stream);
 
+/* ---------------------------------------------------------------- pass 3: point fusion */
+
+typedef struct mvs_fuse_args {
+    int32_t H, W;
+    const float* depth;                    /* (H, W) the view's final depth map, NaN = none     */
+    const uint8_t* used;                   /* (H, W) the view's used mask (read)                */
+    const double* cam;                     /* host, 18 doubles: the view's camera row           */
+    int32_t n_nb;                          /* neighbours with a depth map, in the view's order  */
+    int32_t point_stride;                  /* candidates on the stride grid (<= 1: every pixel) */
+    const float* nb_depth[MVS_MAX_SOURCES];
+    uint8_t* nb_used[MVS_MAX_SOURCES];     /* neighbours' used masks (written: 1 where marked)  */
+    int32_t nb_h[MVS_MAX_SOURCES], nb_w[MVS_MAX_SOURCES];
+    const double* nb_cam;                  /* host, n_nb x 18 camera rows                       */
+    const double* rel_tol;                 /* host, n_nb relative depth tolerances              */
+    double px_tol;                         /* forward-backward reprojection tolerance, pixels   */
+    int32_t min_views, pad_;
+    uint8_t* keep;                         /* out (H, W): 1 = the pixel emits a fused point     */
+    double* xyz;                           /* out (3, H, W) float64 fused point where keep      */
+    int32_t* count;                        /* out (H, W) agreeing views + 1 (0 = no candidate)  */
+} mvs_fuse_args;
+
+/* One reference image of the point fusion (densify._fuse_loop, densify.py:688-762, on the
+ * compiled path _fast.ref_points / neighbour_sample / agreement / accumulate,
+ * _fast.pyx:201-284): candidates are the finite pixels not yet used, on the stride grid; each
+ * accumulates the back-projected points of the neighbours that pass the forward-backward check
+ * (in neighbour order) onto its own, is kept with at least min_views views (xyz = sum / count)
+ * and marks the agreeing neighbours' stride-grid pixels as used. Views must be fused one call
+ * after another in the reference's order (sorted view index) on one stream. Bit-exact. */
+mvs_status mvs_fuse_view(const mvs_fuse_args* args, void* stream);
+
 /* ---------------------------------------------------------------- misc */
 
 /* Message of this thread's last failing call ("" if none). Returns the message length. */

@@ -16,6 +16,9 @@
  *                              counter-based draws of libmvs_b200's PatchMatch (rng = 1)
  *   oracle_consistency      <- densify._consistency     (densify.py:441-478; _fast.pyx:201-268)
  *   oracle_init_normals     <- densify._init_normals    (densify.py:481-496)
+ *   oracle_fuse_view        <- one reference image of densify._fuse_loop (densify.py:688-762;
+ *                              _fast.ref_points / neighbour_sample / agreement / accumulate,
+ *                              _fast.pyx:201-284)
  * plus an all-float64 variant of the sweep (oracle_sweep_fp64) used as the precision reference:
  * every sum, NCC, score and the parabola in double, no float32 rounding anywhere.
  *
@@ -811,6 +814,83 @@ EXPORT void oracle_init_normals(int H, int W, const float* D, const float* ray, 
             if (s > 0.0f)
                 for (k = 0; k < 3; k++) n[k] = -n[k];
             for (k = 0; k < 3; k++) normal[k * HW + idx] = n[k];
+        }
+    }
+}
+
+/* One reference image k of densify._fuse_loop (densify.py:688-762) on its compiled path
+ * (_fast.ref_points, neighbour_sample, agreement, accumulate; _fast.pyx:201-284):
+ * candidates are the finite, not yet used pixels of D on the point_stride grid (rows and columns
+ * multiples of the stride); for each the world point X (acc starts at X, cnt at 1), then for
+ * every neighbour j in order the forward-backward check of oracle_consistency, adding j's
+ * back-projected point to acc (component by component) when it agrees. Pixels with
+ * cnt >= min_views are kept: keep = 1, xyz = acc / cnt, and for every agreeing neighbour the
+ * stride-grid pixel ((vi / st) st, (ui / st) st) of j's used mask is set. Outputs: keep (H, W),
+ * xyz (3, H, W) (where keep), count (H, W). */
+EXPORT void oracle_fuse_view(int H, int W, const float* D, uint8_t* used, const double* cam, int n_nb,
+                             const float* const* nb_depth, uint8_t* const* nb_used, const int* nb_h, const int* nb_w,
+                             const double* nb_cam, const double* rel_tol, double px_tol, int min_views,
+                             int point_stride, uint8_t* keep, double* xyz, int32_t* count)
+{
+    const double* R = cam;
+    const double* C = cam + 9;
+    const int st = point_stride > 1 ? point_stride : 1;
+    const ptrdiff_t HW = (ptrdiff_t)H * W;
+    int y, x, j, i;
+    for (y = 0; y < H; y++) {
+        for (x = 0; x < W; x++) {
+            const ptrdiff_t idx = (ptrdiff_t)y * W + x;
+            const float Dv = D[idx];
+            int64_t ui_[16], vi_[16];
+            int ok_[16];
+            double X[3], acc[3], M[3], rx, ry, d;
+            int32_t cnt = 1;
+            keep[idx] = 0;
+            count[idx] = 0;
+            if (!isfinite(Dv) || used[idx] || (st > 1 && (y % st != 0 || x % st != 0))) continue;
+            d = Dv;
+            undistort((double)x, (double)y, cam, &rx, &ry);
+            M[0] = rx * d; M[1] = ry * d; M[2] = d;
+            for (i = 0; i < 3; i++) X[i] = C[i] + dot3_blas(M[0], M[1], M[2], R[i], R[3 + i], R[6 + i]);
+            for (i = 0; i < 3; i++) acc[i] = X[i];
+            for (j = 0; j < n_nb; j++) {
+                const double* cj = nb_cam + 18 * j;
+                const double* Rj = cj;
+                const double* Cj = cj + 9;
+                double dx[3], xc[3], u, v, dd, xj, yj, Mj[3], Xj[3], dk[3], xk[3], ub, vb;
+                int64_t a, b;
+                for (i = 0; i < 3; i++) dx[i] = X[i] - Cj[i];
+                for (i = 0; i < 3; i++) xc[i] = dot3_blas(dx[0], dx[1], dx[2], Rj[3 * i], Rj[3 * i + 1], Rj[3 * i + 2]);
+                project(xc[0], xc[1], xc[2], cj, &u, &v);
+                a = (int64_t)rint(u);
+                b = (int64_t)rint(v);
+                if (xc[2] > 0 && a >= 0 && b >= 0 && a < nb_w[j] && b < nb_h[j])
+                    dd = nb_depth[j][(ptrdiff_t)b * nb_w[j] + a];
+                else
+                    dd = NAN;
+                undistort((double)a, (double)b, cj, &xj, &yj);
+                Mj[0] = xj * dd; Mj[1] = yj * dd; Mj[2] = dd;
+                for (i = 0; i < 3; i++) Xj[i] = Cj[i] + dot3_blas(Mj[0], Mj[1], Mj[2], Rj[i], Rj[3 + i], Rj[6 + i]);
+                for (i = 0; i < 3; i++) dk[i] = Xj[i] - C[i];
+                for (i = 0; i < 3; i++) xk[i] = dot3_blas(dk[0], dk[1], dk[2], R[3 * i], R[3 * i + 1], R[3 * i + 2]);
+                project(xk[0], xk[1], xk[2], cam, &ub, &vb);
+                ui_[j] = a;
+                vi_[j] = b;
+                {
+                    const double t = rel_tol[j] * dd;
+                    ok_[j] = isfinite(dd) && hypot(ub - (double)x, vb - (double)y) <= px_tol && fabs(dd - xc[2]) <= t;
+                }
+                if (ok_[j]) {
+                    for (i = 0; i < 3; i++) acc[i] = acc[i] + Xj[i];
+                    cnt = cnt + 1;
+                }
+            }
+            count[idx] = cnt;
+            if (cnt < min_views) continue;
+            keep[idx] = 1;
+            for (i = 0; i < 3; i++) xyz[i * HW + idx] = acc[i] / (double)cnt;
+            for (j = 0; j < n_nb; j++)
+                if (ok_[j]) nb_used[j][(ptrdiff_t)((vi_[j] / st) * st) * nb_w[j] + (ui_[j] / st) * st] = 1;
         }
     }
 }

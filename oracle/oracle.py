@@ -62,6 +62,9 @@ def lib() -> C.CDLL:
         L.oracle_consistency.restype = None
         L.oracle_consistency.argtypes = [C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp,
                                          C.c_double, C.c_int, vp]
+        L.oracle_fuse_view.restype = None
+        L.oracle_fuse_view.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, C.c_double,
+                                       C.c_int, C.c_int, vp, vp, vp]
         L.oracle_init_normals.restype = None
         L.oracle_init_normals.argtypes = [C.c_int, C.c_int, vp, vp, vp]
         L.oracle_pm_uniform.argtypes = [C.c_uint32, C.c_int, C.c_int64, C.c_int]
@@ -303,3 +306,40 @@ def init_normals(D, ray) -> np.ndarray:
     out = np.empty((3, H, W), np.float32)
     lib().oracle_init_normals(H, W, _p(D), _p(_f32(ray)), _p(out))
     return out
+
+
+def fuse(order, maps, cams, nbrs, rel_tols, px_tol, min_views, point_stride, rgbs):
+    """densify._fuse (densify.py:676-762) restated: views in `order`, each fused against its
+    neighbours (nbrs[k], rel_tols[k][j]) with the used masks of the views carried from one view to
+    the next. maps[k]: float32 depth (NaN = none); rgbs[k]: (H, W, 3) uint8. Returns
+    (xyz float64 (n, 3), cols uint8 (n, 3), nv uint8 (n,), owner int32 (n,), used {k: bool})."""
+    used = {k: np.zeros(maps[k].shape, np.uint8) for k in maps}
+    pts, cols, nv, owner = [], [], [], []
+    for k in order:
+        D = _f32(maps[k])
+        H, W = D.shape
+        nb = [j for j in nbrs[k] if j in maps]
+        n = len(nb)
+        nmaps = [_f32(maps[j]) for j in nb]
+        mp = (C.c_void_p * max(n, 1))(*[m.ctypes.data for m in nmaps])
+        up = (C.c_void_p * max(n, 1))(*[used[j].ctypes.data for j in nb])
+        hs = np.array([m.shape[0] for m in nmaps] or [0], np.int32)
+        ws = np.array([m.shape[1] for m in nmaps] or [0], np.int32)
+        rows = _f64(np.array([cam_row(cams[j]) for j in nb], np.float64).reshape(-1))
+        tol = _f64(np.array([rel_tols[k][j] for j in nb], np.float64).reshape(-1))
+        keep = np.zeros((H, W), np.uint8)
+        xyz = np.zeros((3, H, W), np.float64)
+        cnt = np.zeros((H, W), np.int32)
+        lib().oracle_fuse_view(H, W, _p(D), _p(used[k]), _p(_f64(cam_row(cams[k]))), n, mp, up, _p(hs), _p(ws),
+                               _p(rows), _p(tol), float(px_tol), int(min_views), int(point_stride), _p(keep),
+                               _p(xyz), _p(cnt))
+        vv, uu = np.nonzero(keep)
+        if len(vv) == 0:
+            continue
+        pts.append(xyz[:, vv, uu].T.copy())
+        cols.append(rgbs[k][vv, uu])
+        nv.append(np.minimum(cnt[vv, uu], 255).astype(np.uint8))
+        owner.append(np.full(len(vv), k, np.int32))
+    cat = lambda a, shape, dt: np.concatenate(a) if a else np.zeros(shape, dt)
+    return (cat(pts, (0, 3), np.float64), cat(cols, (0, 3), np.uint8), cat(nv, (0,), np.uint8),
+            cat(owner, (0,), np.int32), {k: u.astype(bool) for k, u in used.items()})

@@ -60,6 +60,14 @@ class ConsArgs(C.Structure):
                 ("score", vp), ("min_ncc", C.c_double), ("min_views", i32), ("pad2_", i32), ("active", vp)]
 
 
+class FuseArgs(C.Structure):
+    _fields_ = [("H", i32), ("W", i32), ("depth", vp), ("used", vp), ("cam", vp), ("n_nb", i32),
+                ("point_stride", i32), ("nb_depth", vp * MAX_SOURCES), ("nb_used", vp * MAX_SOURCES),
+                ("nb_h", i32 * MAX_SOURCES), ("nb_w", i32 * MAX_SOURCES), ("nb_cam", vp), ("rel_tol", vp),
+                ("px_tol", C.c_double), ("min_views", i32), ("pad_", i32), ("keep", vp), ("xyz", vp),
+                ("count", vp)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("sweep", SweepArgs), ("depth", vp)]
 
@@ -95,6 +103,7 @@ SIGNATURES = {
     "mvs_server_destroy": (None, [vp]),
     "mvs_consistency": (i32, [vp, vp]),
     "mvs_init_normals": (i32, [i32, i32, vp, vp, vp, vp]),
+    "mvs_fuse_view": (i32, [vp, vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_version": (C.c_char_p, []),
 }

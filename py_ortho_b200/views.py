@@ -21,6 +21,7 @@ reference's pass 2 reads it).
 """
 from __future__ import annotations
 
+import ctypes
 from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
@@ -180,6 +181,60 @@ def repair(k: int, raw: Dict[int, torch.Tensor], score: torch.Tensor, low: torch
                                       k * 2654435761 % 2**32, precision=getattr(opt, "pm_precision", "fp64"))
     D = torch.where((S < opt.min_ncc) | low, torch.full_like(D, float("nan")), D)
     return D, changed, n_active
+
+
+# ------------------------------------------------------------------ pass 3: point fusion
+def fuse(order: Sequence[int], maps: Dict[int, object], cams, nbrs, rel_tols, px_tol: float, min_views: int,
+         point_stride: int, rgbs):
+    """Point fusion of the final depth maps (densify._fuse, densify.py:676-762) on the device:
+    views in `order` (the reference fuses sorted(have)), one ``mvs_fuse_view`` launch each, the
+    used masks carried from view to view on the device. maps[k]: (H, W) depth (NaN = none);
+    nbrs[k]: neighbour ids; rel_tols[k][j]: relative depth tolerance; rgbs[k]: (H, W, 3) uint8.
+    Returns (xyz float64 (n, 3), colours uint8 (n, 3), views uint8 (n,), owner int32 (n,)) as
+    torch CUDA tensors in the reference's order (views in order, pixels row-major), and the
+    used masks {k: bool tensor}."""
+    dev = L.require_cuda()
+    lib = L.load()
+    D = {k: _dev32(m, dev) for k, m in maps.items()}
+    used = {k: torch.zeros(tuple(D[k].shape), dtype=torch.uint8, device=dev) for k in D}
+    pts, cols, nv, owner = [], [], [], []
+    sh = L.stream_handle()
+    for k in order:
+        if k not in D:
+            continue
+        H, W = (int(v) for v in D[k].shape)
+        nb = [j for j in nbrs[k] if j in D and j != k]
+        if len(nb) > L.MAX_SOURCES:
+            raise ValueError(f"fuse: view {k} has {len(nb)} neighbours (at most {L.MAX_SOURCES})")
+        cam = L.host_f64(cam_row(cams[k]))
+        nb_cam = L.host_f64(np.array([cam_row(cams[j]) for j in nb], np.float64).reshape(-1) if nb else np.zeros(1))
+        tol = L.host_f64(np.array([rel_tols[k][j] for j in nb], np.float64) if nb else np.zeros(1))
+        keep = torch.empty((H, W), dtype=torch.uint8, device=dev)
+        xyz = torch.empty((3, H, W), dtype=torch.float64, device=dev)
+        cnt = torch.empty((H, W), dtype=torch.int32, device=dev)
+        a = L.FuseArgs()
+        a.H, a.W, a.depth, a.used, a.cam = H, W, D[k].data_ptr(), used[k].data_ptr(), L.host_ptr(cam)
+        a.n_nb, a.point_stride = len(nb), int(point_stride)
+        for i, j in enumerate(nb):
+            a.nb_depth[i], a.nb_used[i] = D[j].data_ptr(), used[j].data_ptr()
+            a.nb_h[i], a.nb_w[i] = int(D[j].shape[0]), int(D[j].shape[1])
+        a.nb_cam, a.rel_tol, a.px_tol, a.min_views = L.host_ptr(nb_cam), L.host_ptr(tol), float(px_tol), int(min_views)
+        a.keep, a.xyz, a.count = keep.data_ptr(), xyz.data_ptr(), cnt.data_ptr()
+        L.check(lib.mvs_fuse_view(ctypes.addressof(a), sh), "fuse")
+        sel = torch.nonzero(keep.view(-1)).squeeze(1)          # row-major, as np.nonzero
+        if sel.numel() == 0:
+            continue
+        pts.append(xyz.view(3, -1)[:, sel].T)
+        rgb = torch.as_tensor(np.ascontiguousarray(rgbs[k]), device=dev) if not isinstance(rgbs[k], torch.Tensor) \
+            else rgbs[k].to(dev)
+        cols.append(rgb.reshape(-1, 3)[sel])
+        nv.append(cnt.view(-1)[sel].clamp(max=255).to(torch.uint8))
+        owner.append(torch.full((sel.numel(),), k, dtype=torch.int32, device=dev))
+
+    def cat(a, shape, dt):
+        return torch.cat(a) if a else torch.zeros(shape, dtype=dt, device=dev)
+    return (cat(pts, (0, 3), torch.float64), cat(cols, (0, 3), torch.uint8), cat(nv, (0,), torch.uint8),
+            cat(owner, (0,), torch.int32), {k: u.bool() for k, u in used.items()})
 
 
 # ------------------------------------------------------------------ sharding and the exchange

@@ -24,6 +24,7 @@ Fixtures (each .npz holds the inputs and the reference outputs):
                      (depth maps, geometric consistency, PatchMatch repair with the neighbours'
                      depth maps, final filter), recording what the reference's own
                      _consistency, _init_normals and _dense.pm_refine received and returned
+  fuse_case.npz    - densify._fuse (point fusion) on views_case's pass-2 maps, in two settings
 """
 from __future__ import annotations
 
@@ -433,6 +434,45 @@ def views_case(D, W=160, H=120):
     shutil.rmtree(out_dir, ignore_errors=True)
 
 
+def fuse_case(D):
+    """The reference's point fusion (densify._fuse, densify.py:676-762, through its compiled path
+    _fast.ref_points / neighbour_sample / agreement / accumulate) on the pass-2 depth maps of
+    views_case.npz, in two settings: (min_views, point_stride) = (2, 2) and (3, 1)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from types import SimpleNamespace
+    z = np.load(os.path.join(HERE, "views_case.npz"))
+    f, cx, cy, W, H = (float(v) for v in z["intr"])
+    W, H = int(W), int(H)
+    have = [int(k) for k in z["have"]]
+    N = len(z["C"])
+    cams = {k: D._Cam(z["R"][k], z["C"][k], f, 0.0, 0.0, cx, cy, W, H) for k in range(N)}
+    nbrs = {k: [int(j) for j in z[f"nbrs{k}"]] for k in have}
+    tols = {k: {j: float(t) for j, t in zip(nbrs[k], z[f"tol{k}"])} for k in have}
+    px_tol = float(z["px_tol"])
+    rgb = {k: np.ascontiguousarray(np.repeat(z[f"img{k}"][:, :, None], 3, axis=2)) for k in range(N)}
+    res = {"px_tol": np.array(px_tol)}
+    for c, (min_views, stride) in enumerate(((2, 2), (3, 1))):
+        dm = {k: np.ascontiguousarray(z[f"final{k}"], np.float32) for k in have}
+        used = {k: np.zeros(dm[k].shape, bool) for k in have}
+        pts, cols, nv, owner = [], [], [], []
+        opt = SimpleNamespace(point_stride=stride, neighbors=4)
+        fpool = ThreadPoolExecutor(1)
+        try:
+            D._fuse(sorted(have), dm, used, cams, nbrs, set(have), lambda k: tols[k], opt, px_tol, min_views,
+                    lambda k: (None, rgb[k], None), {}, pts, cols, nv, owner, 1000, fpool)
+        finally:
+            fpool.shutdown()
+        res[f"f{c}_args"] = np.array([min_views, stride], np.int64)
+        res[f"f{c}_xyz"] = np.concatenate(pts) if pts else np.zeros((0, 3))
+        res[f"f{c}_cols"] = np.concatenate(cols) if cols else np.zeros((0, 3), np.uint8)
+        res[f"f{c}_nv"] = np.concatenate(nv) if nv else np.zeros(0, np.uint8)
+        res[f"f{c}_owner"] = np.concatenate(owner) if owner else np.zeros(0, np.int32)
+        for k in have:
+            res[f"f{c}_used{k}"] = used[k]
+        print(f"fuse_case {c}: {len(res[f'f{c}_xyz'])} points")
+    np.savez_compressed(os.path.join(HERE, "fuse_case.npz"), **res)
+
+
 def main():
     D = refpkg.load_densify()
     R = O.reference()
@@ -445,6 +485,7 @@ def main():
     pm_case(R)
     depth_map_case(D)
     views_case(D)
+    fuse_case(D)
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -39,7 +39,8 @@ def test_library_exports_every_declared_function():
 def test_ctypes_structs_match_the_c_layout(tmp_path):
     L = _lib()
     structs = {"mvs_hyp": L.Hyp, "mvs_sweep_args": L.SweepArgs, "mvs_pm_args": L.PMArgs,
-               "mvs_batch_job": L.BatchJob, "mvs_batch_tuning": L.BatchTuning}
+               "mvs_batch_job": L.BatchJob, "mvs_batch_tuning": L.BatchTuning,
+               "mvs_consistency_args": L.ConsArgs, "mvs_fuse_args": L.FuseArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')

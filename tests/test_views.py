@@ -7,11 +7,12 @@ import os
 import socket
 
 import numpy as np
+import pytest
 import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
-from conftest import same_bits
+from conftest import golden, same_bits
 from oracle import oracle as O
 from tests_support import views_fixture
 from py_ortho_b200 import views as V
@@ -152,3 +153,32 @@ def test_run_passes_two_ranks_gloo_matches_one_rank():
         assert all(owner[k] == rank for k in out)                   # each view on its owner only
         merged.update(out)
     assert merged == single
+
+
+# ------------------------------------------------------------------ point fusion (densify._fuse)
+def _fuse_inputs(z, fz, c):
+    from tests_support import views_fixture
+    _, rec, cams, greys = views_fixture()
+    have = [int(k) for k in z["have"]]
+    maps = {k: np.ascontiguousarray(z[f"final{k}"], np.float32) for k in have}
+    nbrs = {k: [int(j) for j in z[f"nbrs{k}"]] for k in have}
+    tols = {k: {j: float(t) for j, t in zip(nbrs[k], z[f"tol{k}"])} for k in have}
+    rgbs = {k: np.ascontiguousarray(np.repeat(z[f"img{k}"][:, :, None], 3, axis=2)) for k in range(len(cams))}
+    min_views, stride = (int(v) for v in fz[f"f{c}_args"])
+    return sorted(have), maps, cams, nbrs, tols, float(fz["px_tol"]), min_views, stride, rgbs
+
+
+@pytest.mark.parametrize("c", [0, 1])
+def test_oracle_fuse_matches_the_reference(c):
+    """The oracle's fusion reproduces the reference's densify._fuse bit for bit: every fused point,
+    colour, view count and owner, in the reference's order, and the used masks it leaves."""
+    z, fz = golden("views_case.npz"), golden("fuse_case.npz")
+    order, maps, cams, nbrs, tols, px_tol, min_views, stride, rgbs = _fuse_inputs(z, fz, c)
+    xyz, cols, nv, owner, used = O.fuse(order, maps, cams, nbrs, tols, px_tol, min_views, stride, rgbs)
+    assert len(xyz) == len(fz[f"f{c}_xyz"]) > 0
+    assert same_bits(xyz, fz[f"f{c}_xyz"])
+    assert np.array_equal(cols, fz[f"f{c}_cols"])
+    assert np.array_equal(nv, fz[f"f{c}_nv"])
+    assert np.array_equal(owner, fz[f"f{c}_owner"])
+    for k in order:
+        assert np.array_equal(used[k], fz[f"f{c}_used{k}"])

@@ -2,13 +2,14 @@
 PatchMatch mask (mvs_consistency) and the initial normals (mvs_init_normals) bit for bit, the
 pass-2 PatchMatch repair bit for bit against the oracle with the same counter-based draws, and
 passes 1 + 2 end to end (py_ortho_b200.views.densify_views) against the reference's final
-depth maps."""
+depth maps, and the point fusion (mvs_fuse_view) against the reference's densify._fuse."""
 import numpy as np
 import pytest
 import torch
 
-from conftest import same_bits
+from conftest import golden, same_bits
 from tests_support import views_fixture
+from py_ortho_b200 import views as V
 
 pytestmark = pytest.mark.gpu
 
@@ -104,3 +105,20 @@ def test_densify_views_end_to_end_against_reference():
         assert (fin == rfin).mean() > 0.95
         assert np.median(rel) < 1e-3
         assert (rel <= 1e-3).mean() > 0.8
+
+
+@pytest.mark.parametrize("c", [0, 1])
+def test_fuse_bit_exact_vs_reference(c):
+    """mvs_fuse_view, view after view: the reference's densify._fuse output bit for bit (points,
+    colours, view counts, owners, order) and the used masks it leaves."""
+    from test_views import _fuse_inputs
+    z, fz = golden("views_case.npz"), golden("fuse_case.npz")
+    order, maps, cams, nbrs, tols, px_tol, min_views, stride, rgbs = _fuse_inputs(z, fz, c)
+    xyz, cols, nv, owner, used = V.fuse(order, maps, cams, nbrs, tols, px_tol, min_views, stride, rgbs)
+    assert xyz.shape[0] == len(fz[f"f{c}_xyz"]) > 0
+    assert same_bits(xyz.cpu().numpy(), fz[f"f{c}_xyz"])
+    assert np.array_equal(cols.cpu().numpy(), fz[f"f{c}_cols"])
+    assert np.array_equal(nv.cpu().numpy(), fz[f"f{c}_nv"])
+    assert np.array_equal(owner.cpu().numpy(), fz[f"f{c}_owner"])
+    for k in order:
+        assert np.array_equal(used[k].cpu().numpy(), fz[f"f{c}_used{k}"])
