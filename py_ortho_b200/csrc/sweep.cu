@@ -9,8 +9,8 @@ __global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ Sw
     extern __shared__ float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, KMAX, PLANES, F16>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb, p.rec ? (int)blockIdx.z : -1,
-                                     reinterpret_cast<float*>(smem4));
+    sweep_tile<R, KMAX, PLANES, F16, true>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb, p.rec ? (int)blockIdx.z : -1,
+                                           reinterpret_cast<float*>(smem4));
 }
 
 __global__ void merge_kernel(long long HW, int nchunks, int i0, int i1, int ppc, const float* __restrict__ rec,

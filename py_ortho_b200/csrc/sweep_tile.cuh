@@ -324,6 +324,9 @@ __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4
         a2 = __fadd_rn(a2, s2[t]);
         a3 = __fadd_rn(a3, s3[t]);
     }
+    // hs_index(hy, P sg + j) = hy TW + P sg + (j ^ kx): the segment's columns share (col >> 4) = sg
+    float4* row = sH + hy * TW + P * sg;
+    const int kx = (sg + hy) & 7;
 #pragma unroll
     for (int j = 0; j < P; ++j) {
         if (j > 0) {
@@ -333,7 +336,7 @@ __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4
             a2 = __fadd_rn(a2, __fsub_rn(s2[tn], s2[to]));
             a3 = __fadd_rn(a3, __fsub_rn(s3[tn], s3[to]));
         }
-        sH[hs_index(hy, P * sg + j)] = make_float4(a0, a1, a2, a3);
+        row[j ^ kx] = make_float4(a0, a1, a2, a3);
     }
 }
 
@@ -344,10 +347,16 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
                                         float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
     constexpr int K = 2 * R + 1;
     const float k2 = (float)(K * K), inv_k2 = 1.0f / (float)(K * K);
+    // y0 is a multiple of 8 (ROWS = 8), so hs_index(y0 + t, c) = (y0 + t) TW + sw[t & 7]
+    static_assert(ROWS % 8 == 0, "stage C rows must start on a multiple of 8");
+    int sw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
+    const float4* col = sH + y0 * TW;
     float cv = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
 #pragma unroll
     for (int t = 0; t < K; ++t) {
-        const float4 h = sH[hs_index(y0 + t, c)];
+        const float4 h = col[t * TW + sw[t & 7]];
         if constexpr (WITHV) cv = __fadd_rn(cv, h.x);
         cj = __fadd_rn(cj, h.y);
         cjj = __fadd_rn(cjj, h.z);
@@ -356,8 +365,8 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 #pragma unroll
     for (int j = 0; j < ROWS; ++j) {
         if (j > 0) {
-            const float4 hn = sH[hs_index(y0 + j + 2 * R, c)];
-            const float4 ho = sH[hs_index(y0 + j - 1, c)];
+            const float4 hn = col[(j + 2 * R) * TW + sw[(j + 2 * R) & 7]];
+            const float4 ho = col[(j - 1) * TW + sw[(j - 1) & 7]];
             if constexpr (WITHV) cv = __fadd_rn(cv, __fsub_rn(hn.x, ho.x));
             cj = __fadd_rn(cj, __fsub_rn(hn.y, ho.y));
             cjj = __fadd_rn(cjj, __fsub_rn(hn.z, ho.z));
@@ -390,7 +399,9 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 // One tile x hypothesis range at window radius R. `chunk` >= 0 writes the chunk record `chunk`
 // of p.nchunks instead of the caller's state. Explicit _rn arithmetic in stages B and C fixes
 // every rounding, so the result never depends on how the compiler scheduled this instance.
-template <int R, int KMAX, bool PLANES, bool F16>
+// WIDE: interior tiles gather all of a thread's warp samples before storing any (more loads in
+// flight; more registers - the single-view kernel, whose radius is a template argument, uses it).
+template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false>
 __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
     using G = Geom<R>;
     constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
@@ -463,7 +474,28 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             if constexpr (PLANES) {
                 const Coef cf = sC[s];
                 constexpr int PER = (HR * HC + NT - 1) / NT;
-                if (cf.inside && tile_inside) {
+                if (WIDE && cf.inside && tile_inside) {
+                    // every sample of the thread gathered before any is stored (the surplus of the
+                    // last round repeats the tile's last sample and is not stored): the gathers
+                    // are independent and in flight together
+                    float Jv[PER];
+                    int off[PER];
+#pragma unroll
+                    for (int k = 0; k < PER; ++k) {
+                        const int e0 = tid + k * NT;
+                        const int e = e0 < HR * HC ? e0 : HR * HC - 1;
+                        const int hy = e / HC, hc = e - hy * HC;
+                        Jv[k] = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
+                        off[k] = e0 < HR * HC ? hy * JP + (RA - R) + hc : -1;
+                    }
+#pragma unroll
+                    for (int k = 0; k < PER; ++k) {
+                        if (off[k] >= 0) {
+                            any_invalid |= Jv[k] != Jv[k];
+                            sJ[off[k]] = Jv[k];
+                        }
+                    }
+                } else if (cf.inside && tile_inside) {
 #pragma unroll 4
                     for (int k = 0; k < PER; ++k) {
                         const int e = tid + k * NT;
