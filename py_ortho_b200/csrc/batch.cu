@@ -29,6 +29,14 @@ struct JobFin {                        // per-job table of the merge / finalize 
     float* depth;
 };
 
+// One radius of the tile engine as an out-of-line call: the persistent kernel dispatches on the
+// work item's radius, and keeping each instance out of line gives each its own register
+// allocation (inlined together, the largest instance's pressure spilled the others).
+template <int R, int KMAX, bool F16, bool WIDE>
+__device__ __noinline__ void batch_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int ch, float* smem) {
+    sweep_tile<R, KMAX, true, F16, WIDE>(p, tx, ty, pa, pb, ch, smem);
+}
+
 template <int RMAX, int KMAX, bool F16>
 __global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restrict__ jobs, const int4* __restrict__ items,
                                                       int n_items, int* counter) {
@@ -50,17 +58,17 @@ __global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restr
         const int tx = w.y * TW, ty = w.z * TH;
         // the radius is uniform per work item: each case is the single-view instance itself
         switch (p.r) {
-            case 0: sweep_tile<0, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-            case 1: sweep_tile<1, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-            case 2: sweep_tile<2, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-            case 3: sweep_tile<3, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+            case 0: batch_tile<0, KMAX, F16, false>(p, tx, ty, pa, pb, ch, smem); break;
+            case 1: batch_tile<1, KMAX, F16, false>(p, tx, ty, pa, pb, ch, smem); break;
+            case 2: batch_tile<2, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+            case 3: batch_tile<3, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
             default:
                 if constexpr (RMAX > 3) {
                     switch (p.r) {
-                        case 4: sweep_tile<4, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-                        case 5: sweep_tile<5, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-                        case 6: sweep_tile<6, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
-                        default: sweep_tile<7, KMAX, true, F16>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 4: batch_tile<4, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 5: batch_tile<5, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 6: batch_tile<6, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+                        default: batch_tile<7, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
                     }
                 }
         }

@@ -294,7 +294,9 @@ __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4
     using G = Geom<R>;
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
-    const int hy = tid / NSEG, sg = tid - hy * NSEG;
+    // consecutive threads take consecutive rows of one segment: a quarter-warp's 16-byte loads then
+    // start (19 hy + 4 sg) mod 8 float4 units into the bank space - 8 distinct groups (JP = 76)
+    const int sg = tid / HR, hy = tid - sg * HR;
     const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
     const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
     float v[NIN], s1[NIN], s2[NIN], s3[NIN];
