@@ -361,6 +361,9 @@ __global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_con
 #ifndef PM_LANE_MIN_BLOCKS
 #define PM_LANE_MIN_BLOCKS 3
 #endif
+#ifndef PM_UNIT_INLINE
+#define PM_UNIT_INLINE __forceinline__
+#endif
 
 __device__ __forceinline__ int pmf_floor(float x, float& f) {   // |x| < 2^22
     const float t = __fadd_rd(x, 12582912.0f);
@@ -442,8 +445,8 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
 // (s < S); n . ray_p = ndr < -1e-6. Follows _pm_cost: -1 below the count gate, 0 below the
 // variance floor.
 template <int NSIDE>
-__device__ float pm_unit_ncc(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
-                             const double* n, double ndr, int sl) {
+__device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
+                                            const double* n, double ndr, int sl) {
     const double num = d * ndr;
     const float n0 = (float)n[0], n1 = (float)n[1], n2 = (float)n[2], denp = (float)ndr;
     const int NW = NSIDE > 0 ? NSIDE * NSIDE : wn.nw;
