@@ -336,6 +336,12 @@ mvs_status mvs_fuse_view(const mvs_fuse_args* args, void* stream);
 
 /* ---------------------------------------------------------------- misc */
 
+/* Device-side waits that gave up since the last call (the sweep's TMA copy of the reference
+ * tile waits on an mbarrier with an iteration limit; a tile whose copy never completes leaves its
+ * state untouched and is counted here). Synchronises with the device; clears the count.
+ * Returns MVS_ERR_TIMEOUT when the count was non-zero. No counterpart in the reference. */
+mvs_status mvs_device_faults(uint32_t* count);
+
 /* Message of this thread's last failing call ("" if none). Returns the message length. */
 size_t mvs_last_error(char* buf, size_t cap);
 /* Library version string. */

@@ -105,6 +105,7 @@ SIGNATURES = {
     "mvs_init_normals": (i32, [i32, i32, vp, vp, vp, vp]),
     "mvs_fuse_view": (i32, [vp, vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
+    "mvs_device_faults": (i32, [vp]),
     "mvs_version": (C.c_char_p, []),
 }
 

@@ -1,6 +1,7 @@
 // Shared helpers of libmvs_b200: status / last-error plumbing and small device utilities.
 #pragma once
 
+#include <cuda.h>              // CUtensorMap (the tensor-map type only; the driver is reached at run time)
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <stdint.h>

@@ -2,15 +2,51 @@
 // plane-chunk merge and the sub-hypothesis parabola (finalize), plus their C-ABI entry points.
 #include "sweep_tile.cuh"
 
+#include <cudaTypedefs.h>
+#include <mutex>
+
 namespace mvs {
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// The reference's 2D tiled map for the tile copy: box = the tile with its halo (Geom<r>::JP x
+// Geom<r>::HR floats). Needs a 16-byte aligned base and a row pitch that is a multiple of 16
+// bytes (W % 4 == 0); otherwise the tile is loaded by the threads (same values).
+static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r) {
+    PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+    if (!enc || !ref || (reinterpret_cast<uintptr_t>(ref) & 15u) || W % 4 != 0 || W < 1 || H < 1) return false;
+    const int RA = (r + 3) & ~3;
+    const cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
+    const cuuint64_t strides[1] = {(cuuint64_t)W * sizeof(float)};
+    const cuuint32_t box[2] = {(cuuint32_t)(TW + 2 * RA + 4), (cuuint32_t)(TH + 2 * r)};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult e = enc(&p.ref_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ref), dims, strides, box,
+                           es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return e == CUDA_SUCCESS;
+}
 
 template <int R, int KMAX, bool PLANES, bool F16>
 __global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ SweepParams p) {
-    extern __shared__ float4 smem4[];
+    extern __shared__ __align__(128) float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, KMAX, PLANES, F16, true>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb, p.rec ? (int)blockIdx.z : -1,
-                                           reinterpret_cast<float*>(smem4));
+    sweep_tile<R, KMAX, PLANES, F16, true, true>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
+                                                 p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
 }
 
 __global__ void merge_kernel(long long HW, int nchunks, int i0, int i1, int ppc, const float* __restrict__ rec,
@@ -219,6 +255,7 @@ mvs_status sweep_range(const mvs_sweep_args* a, int i0, int i1, float* rec_ws, i
         p.hyp_a = a->hyp.maps + (long long)(i0 - a->i0) * p.map_stride;
     }
     p.ppc = (n + nchunks - 1) / nchunks;
+    p.ref_tma = make_ref_map(p, a->ref, a->H, a->W, a->r) ? 1 : 0;
     const int used = (n + p.ppc - 1) / p.ppc;
     p.rec = used > 1 ? rec_ws : nullptr;
     p.nchunks = used;
@@ -328,4 +365,16 @@ extern "C" mvs_status mvs_sweep_finalize(int32_t H, int32_t W, const mvs_hyp* hy
     finalize_kernel<<<(unsigned)((HW + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         H, W, hyp->kind, hyp->n, hyp->t0, a, hyp->step, stride, p0, p1, best, s_prev_best, s_next_best, idx, depth);
     return check_launch("finalize kernel");
+}
+
+extern "C" mvs_status mvs_device_faults(uint32_t* count) {
+    clear_error();
+    unsigned n = 0;
+    MVS_CUDA(cudaMemcpyFromSymbol(&n, g_ref_copy_faults, sizeof(n)), "device faults: read");
+    if (n) {
+        const unsigned zero = 0;
+        MVS_CUDA(cudaMemcpyToSymbol(g_ref_copy_faults, &zero, sizeof(zero)), "device faults: clear");
+    }
+    if (count) *count = n;
+    return n ? fail(MVS_ERR_TIMEOUT, "%u sweep tile(s) gave up waiting for their reference copy", n) : MVS_OK;
 }

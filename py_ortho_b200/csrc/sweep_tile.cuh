@@ -45,6 +45,8 @@ struct SrcGeo {
 };
 
 struct SweepParams {
+    CUtensorMap ref_map;               // 2D tiled map of `ref` (single-view kernel, ref_tma = 1)
+    int ref_tma;                       // 1: the reference tile is copied by TMA
     int H, W, n_src, kk;
     int topk_bottom;                   // 1: keep the n-kk lowest and subtract from the total
     int i0, i1, ppc;                   // hypotheses [i0, i1), planes per chunk
@@ -398,29 +400,85 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
     }
 }
 
+// ---- the reference tile by TMA (single-view kernel): one 2D tiled bulk copy per CTA, completed
+// on an mbarrier. The copy's box is the tile with its halo, JP x HR floats starting at
+// (tx - RA, ty - R): x is a multiple of 4 floats (16 bytes), rows outside the image read as 0,
+// as the per-thread loads give.
+
+// sweeps whose reference-tile copy did not complete within the bounded wait (read and cleared
+// by mvs_device_faults)
+static __device__ unsigned g_ref_copy_faults;
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, unsigned long long* bar,
+                                            unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+// Bounded wait for phase `parity` of an mbarrier: false if it did not complete.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+    for (unsigned it = 0; it < (1u << 20); ++it) {
+        unsigned done;
+        asm volatile(
+            "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+            : "=r"(done)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // One tile x hypothesis range at window radius R. `chunk` >= 0 writes the chunk record `chunk`
 // of p.nchunks instead of the caller's state. Explicit _rn arithmetic in stages B and C fixes
 // every rounding, so the result never depends on how the compiler scheduled this instance.
 // WIDE: interior tiles gather all of a thread's warp samples before storing any (more loads in
 // flight; more registers - the single-view kernel, whose radius is a template argument, uses it).
-template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false>
+// REF_TMA: the reference tile arrives by TMA when p.ref_tma is set (the single-view kernel, whose
+// parameters hold the tensor map; `smem` must then be 128-byte aligned).
+template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false>
 __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
     using G = Geom<R>;
     constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
                   NIN = G::NIN;
-    float* sJ = smem;                                  // HR x JP warped source (NaN = invalid)
-    float* sI = sJ + HR * JP;                          // HR x JP reference (0 outside)
-    float4* sH = reinterpret_cast<float4*>(sI + HR * JP);   // HR x TW (V, J, J^2, J I), swizzled
+    float* sI = smem;                                  // HR x JP reference (0 outside); TMA destination
+    float* sJ = sI + HR * JP;                          // HR x JP warped source (NaN = invalid)
+    float4* sH = reinterpret_cast<float4*>(sJ + HR * JP);   // HR x TW (V, J, J^2, J I), swizzled
     const int H = p.H, W = p.W;
     const int tid = threadIdx.x;
 
     __syncthreads();   // a previous tile of a persistent CTA is done with shared memory
+    bool tma = false;
+    __shared__ __align__(8) unsigned long long s_ref_bar;
+    if constexpr (REF_TMA) {
+        tma = p.ref_tma != 0;
+        if (tma && tid == 0) {
+            mbar_init(&s_ref_bar, 1);
+            tma_load_2d(sI, &p.ref_map, tx - RA, ty - R, &s_ref_bar, (unsigned)(HR * JP * sizeof(float)));
+        }
+    }
     for (int e = tid; e < HR * JP; e += NT) {
-        const int hy = e / JP, hc = e - hy * JP;
-        const int gy = ty - R + hy, gx = tx - RA + hc;
-        float v = 0.f;
-        if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(p.ref + (long long)gy * W + gx);
-        sI[e] = v;
+        if (!tma) {
+            const int hy = e / JP, hc = e - hy * JP;
+            const int gy = ty - R + hy, gx = tx - RA + hc;
+            float v = 0.f;
+            if (gy >= 0 && gy < H && gx >= 0 && gx < W) v = __ldg(p.ref + (long long)gy * W + gx);
+            sI[e] = v;
+        }
         sJ[e] = qnan();
     }
 
@@ -453,6 +511,17 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
     const int nlist = bottom ? nsrc - kk : kk;
     // every halo sample lies inside the reference image (interior tile)
     const bool tile_inside = tx - R >= 0 && ty - R >= 0 && tx + TW + R <= W && ty + TH + R <= H;
+    if constexpr (REF_TMA) {
+        if (tma) {
+            __syncthreads();   // the barrier's initialisation is visible to every thread
+            const bool arrived = mbar_wait_bounded(&s_ref_bar, 0);
+            // a copy that never completed: count it and leave the tile's state untouched
+            if (__syncthreads_or(!arrived)) {
+                if (tid == 0) atomicAdd(&g_ref_copy_faults, 1u);
+                return;
+            }
+        }
+    }
 
     for (int i = pa; i < pb; ++i) {
         float topk[ROWS][KMAX];

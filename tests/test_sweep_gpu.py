@@ -212,3 +212,34 @@ def test_fp16_storage_depth_error_vs_fp64_oracle():
     d64, _, _ = O.sweep_fp64(ref, srcs, z["ray"], z["geo"], hyps64, r, top_k)
     rel = np.abs(d16.cpu().numpy() - d64) / d64
     assert np.median(rel) <= 1e-3
+
+
+def test_reference_tile_by_tma_matches_the_thread_loads():
+    """The single-view sweep copies each tile's reference window by TMA when the image allows it
+    (16-byte aligned base, width a multiple of 4); a reference whose storage starts 4 bytes off
+    takes the per-thread loads. Both give the same bits, and no device wait gave up."""
+    import ctypes
+    from py_ortho_b200 import _lib as L, dense, scene as S
+    from oracle import oracle as O
+    sc = S.make_scene("c1", seed=4, width=128, height=96)
+    ref = sc.grey(sc.ref)
+    srcs = [torch.from_numpy(sc.grey(s)).cuda() for s in sc.srcs]
+    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+    planes = S.plane_list(35.0, 55.0, 24)
+    mu, sd = O.ref_stats(ref, 2)
+    H, W = ref.shape
+    aligned = torch.from_numpy(ref).cuda()
+    buf = torch.empty(H * W + 1, dtype=torch.float32, device="cuda")
+    shifted = buf[1:].view(H, W)
+    shifted.copy_(aligned)
+    assert aligned.data_ptr() % 16 == 0 and shifted.data_ptr() % 16 == 4
+    out = []
+    for r_t in (aligned, shifted):
+        st = dense.sweep(r_t, torch.from_numpy(mu).cuda(), torch.from_numpy(sd).cuda(), None, srcs, geo,
+                         dense.Hypotheses.planes_inv(planes), 2, 2, ref_cam=sc.ref_cam.row())
+        out.append([t.cpu().numpy() for t in st])
+    for a, b in zip(*out):
+        assert same_bits(a, b)
+    n = ctypes.c_uint32(0)
+    L.check(L.load().mvs_device_faults(ctypes.byref(n)), "device faults")
+    assert n.value == 0
