@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--pm-iters", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["headline", "batch", "serve"], default="headline",
+    ap.add_argument("--mode", choices=["headline", "batch", "serve", "fuse", "height"], default="headline",
                     help="headline: the single-view step above; batch: 64 uneven views in one persistent "
                          "launch vs per-view launches; serve: Poisson arrivals through the continuous-batching server")
     ap.add_argument("--jobs", type=int, default=64)
@@ -512,29 +512,32 @@ class _CropCam:
         self.cx, self.cy, self.w, self.h = cam.cx - x0, cam.cy - y0, w, h
 
 
-def flight(dev, seed=0, grid=4, W=4000, H=3000):
+def flight(dev, seed=0, grid=4, W=4000, H=3000, with_depth=False):
     """A seeded grid flight (75 % overlap both ways) of nadir views over one terrain, rendered at
-    W x H on the device: the image pool of the batched / served configurations."""
+    W x H on the device: the image pool of the batched / served configurations (with_depth: also
+    the true camera-axis depth maps)."""
     from py_ortho_b200 import scene as S
     cfg = S.CONFIGS["c2"]
     import dataclasses
     cfg = dataclasses.replace(cfg, forward_overlap=0.75, side_overlap=0.75)
-    fx = W * cfg.altitude / cfg.focal * 0.25
-    fy = H * cfg.altitude / cfg.focal * 0.25
+    f = cfg.focal * W / 4000.0 if with_depth else cfg.focal      # depth flights keep the 4000 px footprint
+    fx = W * cfg.altitude / f * 0.25
+    fy = H * cfg.altitude / f * 0.25
     span_x, span_y = fx * (grid - 1), fy * (grid - 1)
-    terr = S._terrain(cfg, seed, 0.5 * span_x + 0.5 * W * cfg.altitude / cfg.focal + 25.0,
-                      0.5 * span_y + 0.5 * H * cfg.altitude / cfg.focal + 25.0)
-    terr.gsd = cfg.altitude / cfg.focal
+    terr = S._terrain(cfg, seed, 0.5 * span_x + 0.5 * W * cfg.altitude / f + 25.0,
+                      0.5 * span_y + 0.5 * H * cfg.altitude / f + 25.0)
+    terr.gsd = cfg.altitude / f
     att = np.random.default_rng(seed + 7777)
-    cams, imgs = [], []
+    cams, imgs, deps = [], [], []
     for gy in range(grid):
         for gx in range(grid):
             cam = S.Camera(S.attitude(att, 0.3), np.array([gx * fx - 0.5 * span_x, gy * fy - 0.5 * span_y, cfg.altitude]),
-                           cfg.focal, (W - 1) / 2.0, (H - 1) / 2.0, W, H)
-            img, _ = S.render(cam, terr, dev)
+                           f, (W - 1) / 2.0, (H - 1) / 2.0, W, H)
+            img, dep = S.render(cam, terr, dev)
             cams.append(cam)
             imgs.append(img)
-    return cfg, cams, imgs
+            deps.append(dep)
+    return (cfg, cams, imgs, deps) if with_depth else (cfg, cams, imgs)
 
 
 def view_jobs(n_jobs, cams, imgs, dev, seed, prec=None):
@@ -688,12 +691,121 @@ def run_serve(a):
     print(json.dumps(line), flush=True)
 
 
+def run_fuse(a):
+    """Point fusion (densify._fuse, the consumer of the depth maps) of a 4 x 4 grid flight's depth
+    maps on the device: true depths with 0.2 % noise and 2 % holes, 4 nearest neighbours, stride 2,
+    min_views 2. Timed with CUDA events around the whole view-by-view fusion (the per-view
+    compaction included); the C oracle on the first views, per candidate pixel, is the CPU
+    baseline."""
+    import torch
+    from oracle import oracle as O
+    from py_ortho_b200 import views as V
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    W, H = a.width or 2000, a.height or 1500
+    cfg, cams, imgs, deps = flight(dev, a.seed, W=W, H=H, with_depth=True)
+    rng = np.random.default_rng(a.seed)
+    maps = {}
+    for k, d in enumerate(deps):
+        d = (d * (1.0 + rng.normal(0, 0.002, d.shape))).astype(np.float32)
+        d[rng.random(d.shape) < 0.02] = np.nan
+        maps[k] = d
+    N = len(cams)
+    C = np.array([c.C for c in cams])
+    nbrs = {k: [int(j) for j in np.argsort(np.linalg.norm(C - C[k], axis=1))[1:5]] for k in range(N)}
+    tols = {k: {j: 0.01 for j in nbrs[k]} for k in range(N)}
+    rgbs = {k: np.repeat(imgs[k][:, :, None], 3, axis=2) for k in range(N)}
+    order = list(range(N))
+    args = (order, maps, cams, nbrs, tols, 1.5, 2, 2, rgbs)
+    dmaps = {k: torch.from_numpy(m).to(dev) for k, m in maps.items()}
+    drgb = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev) for k, v in rgbs.items()}
+    for _ in range(max(1, a.warmup)):
+        V.fuse(order, dmaps, cams, nbrs, tols, 1.5, 2, 2, drgb)
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        xyz, cols, nv, owner, used = V.fuse(order, dmaps, cams, nbrs, tols, 1.5, 2, 2, drgb)
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    ms = min(ts)
+    cand = sum(int(np.isfinite(m[::2, ::2]).sum()) for m in maps.values())      # upper bound (before marks)
+    # CPU: the oracle on the first two views, per candidate pixel, extrapolated
+    t0 = time.time()
+    xyz_c, *_ = O.fuse(order[:2], {k: maps[k] for k in maps}, cams, nbrs, tols, 1.5, 2, 2, rgbs)
+    cpu_s = time.time() - t0
+    cand2 = sum(int(np.isfinite(maps[k][::2, ::2]).sum()) for k in order[:2])
+    line = {"mode": "fuse", "metric": "fused candidate pixels/s", "unit": "Mpix/s", "views": N, "width": W,
+            "height": H, "ms": round(ms, 2), "value": cand / (ms / 1e3) / 1e6, "points": int(xyz.shape[0]),
+            "cpu_baseline": {"value": cand2 / cpu_s / 1e6, "unit": "Mpix/s", "cores": 1, "kind": "port",
+                             "sample": "oracle_fuse_view on the first 2 views (all their candidates)"},
+            "config": {"workload": "4x4 grid flight, 75 % overlap, depth maps = truth x (1 + N(0, 0.002)), "
+                                   "2 % holes; 4 neighbours, px_tol 1.5, rel_tol 0.01, min_views 2, stride 2"}}
+    print(json.dumps(line), flush=True)
+
+
+def run_height(a):
+    """The legacy ground-grid height sweep (mvs.dense_reconstruct) of a 3 x 3 grid flight on the
+    device, end to end (view loading and pyramids, per-tile sweeps with SGM, colour, blending),
+    timed with CUDA events; the reference's CPU backend ran the same pipeline in the tests."""
+    import torch
+    from types import SimpleNamespace
+    from py_ortho_b200 import height as Hs
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    W, H = a.width or 1000, a.height or 750
+    cfg, cams, imgs, deps = flight(dev, a.seed, grid=3, W=W, H=H, with_depth=True)
+    rng = np.random.default_rng(a.seed)
+    X = []
+    for c, d in zip(cams, deps):                       # tie points: back-projected depth samples
+        v, u = rng.integers(0, H, 400), rng.integers(0, W, 400)
+        z = d[v, u].astype(np.float64)
+        ray = np.stack([(u - c.cx) / c.f, (v - c.cy) / c.f, np.ones(len(u))])
+        X.append((c.C[:, None] + (c.R.T @ ray) * z).T)
+    X = np.concatenate(X)
+    n = len(cams)
+    intr = [SimpleNamespace(f=float(cams[0].f), cx=float(cams[0].cx), cy=float(cams[0].cy), width=W, height=H,
+                            k1=0.0, k2=0.0, k3=0.0)]
+    rec = SimpleNamespace(used=list(range(n)), intr=intr, cam_group=np.zeros(n, np.int32), X=X,
+                          C=np.array([c.C for c in cams]), R=np.array([c.R for c in cams]))
+    frames = [SimpleNamespace(width=W, height=H, path=k) for k in range(n)]
+    rgb = [np.ascontiguousarray(np.repeat(im[:, :, None], 3, axis=2)) for im in imgs]
+    native = float(cams[0].C[2] / cams[0].f)
+    opt = Hs.DenseOptions(gsd=2 * native)
+    run = lambda: Hs.dense_reconstruct(SimpleNamespace(frames=frames, workers=1), rec, {}, native, opt,
+                                       load_rgb=lambda fr, s: rgb[fr.path] if s == 1.0 else
+                                       rgb[fr.path][::int(round(1 / s)), ::int(round(1 / s))])
+    for _ in range(max(1, a.warmup)):
+        r = run()
+    ts = []
+    for _ in range(a.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = run()
+        torch.cuda.synchronize()
+        ts.append(time.perf_counter() - t0)
+    s = min(ts)
+    cells = int(r.Z.size)
+    line = {"mode": "height", "metric": "DSM cells/s (legacy height sweep, end to end)", "unit": "Mcell/s",
+            "value": cells / s / 1e6, "seconds": round(s, 3), "cells": cells, "grid": list(r.Z.shape),
+            "gsd": r.gsd, "finite": float(np.isfinite(r.Z).mean()), "median_score": float(np.median(r.score)),
+            "config": {"workload": f"3x3 grid flight, {W}x{H}, 75 % overlap, DSM at 2x the native GSD, "
+                                   "levels 3, window 7x7, 6 views, SGM on the coarse level"}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     a = parse()
     if a.impl == "reference":
         run_reference(a)
     elif a.mode == "batch":
         run_batch(a)
+    elif a.mode == "fuse":
+        run_fuse(a)
+    elif a.mode == "height":
+        run_height(a)
     elif a.mode == "serve":
         run_serve(a)
     else:

@@ -334,6 +334,58 @@ typedef struct mvs_fuse_args {
  * after another in the reference's order (sorted view index) on one stream. Bit-exact. */
 mvs_status mvs_fuse_view(const mvs_fuse_args* args, void* stream);
 
+/* ---------------------------------------------------------------- legacy height sweep (mvs.py) */
+
+typedef struct mvs_sample_view_args {
+    int32_t h, w, nch;                     /* image (h, w, nch) float32, device                 */
+    const float* img;
+    const double* cam;                     /* host, 18 doubles: R(9) C(3) f k1 k2 k3 cx cy, in
+                                              the pixel units of img                            */
+    double X0, Y0, gsd;                    /* grid: cell (r, c) at (X0 + (c+.5) gsd, Y0 - (r+.5) gsd) */
+    int32_t D, H, W;                       /* heights Z (D, H, W) float32, device               */
+    const float* Z;
+    float* out;                            /* out (D, H, W, nch) float32: 0 where not valid     */
+    uint8_t* valid;                        /* out (D, H, W)                                     */
+} mvs_sample_view_args;
+
+/* Projects a ground grid at per-cell heights into a view and samples it bilinearly (float64 as
+ * the reference's CPU sampler). Replaces _mvs.sample_view (_mvs.pyx:13-58) / the CuPy kernel
+ * sample_view (_cuda.py:88-124) behind backend.sample_view. Bit-exact with _mvs.sample_view. */
+mvs_status mvs_sample_view(const mvs_sample_view_args* args, void* stream);
+
+/* Float64 summed-area (2r+1)^2 window mean with zero padding of B stacked (H, W) float32 planes.
+ * Replaces _fast.box_sat_mean (_fast.pyx:897-942), the CPU backend's box (backend.py:102-114).
+ * Bit-exact. Allocates its table stream-ordered. */
+mvs_status mvs_box_sat_mean(int32_t B, int32_t H, int32_t W, const float* a, int32_t r, float* out, void* stream);
+
+typedef struct mvs_height_score_args {
+    int32_t V, D, H, W;                    /* views (2..16), hypothesis stack (D, H, W)         */
+    int32_t topk;                          /* mean of the topk largest NCCs                     */
+    int32_t pad_;
+    double full, min_texture, full_texture;   /* compared / divided in float32, as NumPy does  */
+    const float* M;                        /* (V, D, H, W) box(S)                               */
+    const float* S2;                       /* (V, D, H, W) box(S * S)                           */
+    const float* VA;                       /* (V, D, H, W) box(valid)                           */
+    const float* PP;                       /* (V(V-1)/2, D, H, W) box(S_a S_b), np.triu_indices */
+    const float* cxs;                      /* (W) float32 cell-centre X                         */
+    const float* cys;                      /* (H) float32 cell-centre Y                         */
+    const double* cam_xy;                  /* host, V x 2 camera centres (X, Y)                 */
+    float* score;                          /* out (D, H, W)                                     */
+    float* st;                             /* out (V, D, H, W) NCC vs the cell's reference, or NULL */
+    int32_t* ref;                          /* out (D, H, W) reference view, or NULL             */
+} mvs_height_score_args;
+
+/* The photo-consistency of every hypothesis cell (mvs.dense_reconstruct's score_at,
+ * mvs.py:254-304) after the sampling and the box means: nearest fully-valid camera as the cell's
+ * reference, NCC of every other view against it, mean of the topk largest (summed in descending
+ * order), times the reference's texture weight. */
+mvs_status mvs_height_score(const mvs_height_score_args* args, void* stream);
+
+/* Semi-global aggregation of a (D, H, W) float32 cost volume along 8 directions, summed in the
+ * reference's direction order. Replaces _mvs.sgm (_mvs.pyx:98-251); bit-exact. */
+mvs_status mvs_sgm(int32_t D, int32_t H, int32_t W, const float* cost, float P1, float P2, float* agg,
+                   void* stream);
+
 /* ---------------------------------------------------------------- misc */
 
 /* Device-side waits that gave up since the last call (the sweep's TMA copy of the reference

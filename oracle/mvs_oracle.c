@@ -894,3 +894,138 @@ EXPORT void oracle_fuse_view(int H, int W, const float* D, uint8_t* used, const 
         }
     }
 }
+
+/* ------------------------------------------------------------------ legacy height sweep (mvs.py) */
+
+/* _mvs.sample_view (_mvs.pyx:13-58): ground cell (r, c) of a (H, W) grid at height Z[r, c] is
+ * (X0 + (c + .5) gsd, Y0 - (r + .5) gsd, Z); projected with the camera (R row-major, C, f, k1..k3,
+ * cx, cy in img pixels), bilinear in float64 over nch channels of img (h, w, nch) with the last
+ * row / column repeated; out (H, W, nch) is written only where valid (the caller zeroes it). */
+EXPORT void oracle_sample_view(int h, int w, int nch, const float* img, const double* R, const double* C, double f,
+                               double k1, double k2, double k3, double cx, double cy, double X0, double Y0,
+                               double gsd, int H, int W, const float* Z, float* out, uint8_t* valid)
+{
+    int r, c, ch;
+    for (r = 0; r < H; r++) {
+        const double Y = Y0 - (r + 0.5) * gsd;
+        for (c = 0; c < W; c++) {
+            const double X = X0 + (c + 0.5) * gsd;
+            const double dx = X - C[0], dy = Y - C[1], dz = (double)Z[(ptrdiff_t)r * W + c] - C[2];
+            const double zc = R[6] * dx + R[7] * dy + R[8] * dz;
+            double xc, yc, nx, ny, r2, d, u, v, fx, fy;
+            ptrdiff_t x0, y0, x1, y1;
+            valid[(ptrdiff_t)r * W + c] = 0;
+            if (zc <= 1e-6) continue;
+            xc = R[0] * dx + R[1] * dy + R[2] * dz;
+            yc = R[3] * dx + R[4] * dy + R[5] * dz;
+            nx = xc / zc;
+            ny = yc / zc;
+            r2 = nx * nx + ny * ny;
+            d = 1.0 + r2 * (k1 + r2 * (k2 + r2 * k3));
+            u = f * d * nx + cx;
+            v = f * d * ny + cy;
+            if (u < 0 || v < 0 || u > (double)(w - 1) || v > (double)(h - 1)) continue;
+            x0 = (ptrdiff_t)u;
+            y0 = (ptrdiff_t)v;
+            x1 = x0 + 1 < w ? x0 + 1 : x0;
+            y1 = y0 + 1 < h ? y0 + 1 : y0;
+            fx = u - (double)x0;
+            fy = v - (double)y0;
+            for (ch = 0; ch < nch; ch++) {
+                const double a00 = img[(y0 * w + x0) * nch + ch], a01 = img[(y0 * w + x1) * nch + ch];
+                const double a10 = img[(y1 * w + x0) * nch + ch], a11 = img[(y1 * w + x1) * nch + ch];
+                out[((ptrdiff_t)r * W + c) * nch + ch] =
+                    (float)((1 - fy) * ((1 - fx) * a00 + fx * a01) + fy * ((1 - fx) * a10 + fx * a11));
+            }
+            valid[(ptrdiff_t)r * W + c] = 1;
+        }
+    }
+}
+
+/* _fast.box_sat_mean (_fast.pyx:897-942): float64 summed-area mean over a (2r+1)^2 window with
+ * zero padding, B planes of (H, W) float32: column sums down the rows, then a running row total
+ * of those, window = ((S[y+k][x+k] - S[y][x+k]) - S[y+k][x]) + S[y][x], divided by k^2. */
+EXPORT int oracle_box_sat_mean(int B, int H, int W, const float* a, int r, float* out)
+{
+    const int k = 2 * r + 1, PW = W + 2 * r + 1, PH = H + 2 * r + 1;
+    const double denom = (double)k * (double)k;
+    double* col;
+    double* sat;
+    int b, i, x, y;
+    if (r < 0) return -1;
+    if (B == 0 || H == 0 || W == 0) return 0;
+    col = (double*)malloc(sizeof(double) * W);
+    sat = (double*)malloc(sizeof(double) * (size_t)PH * PW);
+    if (!col || !sat) { free(col); free(sat); return -2; }
+    for (b = 0; b < B; b++) {
+        const float* ab = a + (size_t)b * H * W;
+        for (x = 0; x < W; x++) col[x] = 0.0;
+        for (i = 0; i < PH; i++) {
+            const int ay = i - r - 1;
+            double* cur = sat + (size_t)i * PW;
+            double total = 0.0;
+            for (x = 0; x < r + 1; x++) cur[x] = 0.0;
+            for (x = 0; x < W; x++) {
+                const double val = (ay >= 0 && ay < H) ? (double)ab[(size_t)ay * W + x] : 0.0;
+                col[x] = col[x] + val;
+                total = total + col[x];
+                cur[x + r + 1] = total;
+            }
+            for (x = r + 1 + W; x < PW; x++) cur[x] = total;
+        }
+        for (y = 0; y < H; y++) {
+            const double* cur = sat + (size_t)(y + k) * PW;
+            const double* old = sat + (size_t)y * PW;
+            for (x = 0; x < W; x++) {
+                double val = cur[x + k] - old[x + k];
+                val = val - cur[x];
+                val = val + old[x];
+                out[(size_t)b * H * W + (size_t)y * W + x] = (float)(val / denom);
+            }
+        }
+    }
+    free(col);
+    free(sat);
+    return 0;
+}
+
+/* _mvs.sgm (_mvs.pyx:98-251): semi-global aggregation of a (D, H, W) float32 cost volume along the
+ * 8 directions (0,1) (0,-1) (1,0) (-1,0) (1,1) (1,-1) (-1,1) (-1,-1), summed in that order:
+ * L(p, d) = C(p, d) + min(L(q, d), L(q, d+-1) + P1, min_k L(q, k) + P2) - min_k L(q, k), q = p - dir. */
+EXPORT int oracle_sgm(int D, int H, int W, const float* cost, float P1, float P2, float* agg)
+{
+    static const int dirs[8][2] = {{0, 1}, {0, -1}, {1, 0}, {-1, 0}, {1, 1}, {1, -1}, {-1, 1}, {-1, -1}};
+    const size_t HW = (size_t)H * W;
+    float* L = (float*)malloc(sizeof(float) * (size_t)D * HW);
+    int k, yy, xx, d;
+    if (!L) return -2;
+    for (size_t q = 0; q < (size_t)D * HW; q++) agg[q] = 0.0f;
+    for (k = 0; k < 8; k++) {
+        const int dy = dirs[k][0], dx = dirs[k][1];
+        for (yy = 0; yy < H; yy++) {
+            const int y = dy >= 0 ? yy : H - 1 - yy;
+            for (xx = 0; xx < W; xx++) {
+                const int x = dx >= 0 ? xx : W - 1 - xx;
+                const int py = y - dy, px = x - dx;
+                const size_t o = (size_t)y * W + x;
+                if (py < 0 || py >= H || px < 0 || px >= W) {
+                    for (d = 0; d < D; d++) L[d * HW + o] = cost[d * HW + o];
+                } else {
+                    const size_t po = (size_t)py * W + px;
+                    float best = L[po];
+                    for (d = 1; d < D; d++) if (L[d * HW + po] < best) best = L[d * HW + po];
+                    for (d = 0; d < D; d++) {
+                        float v = L[d * HW + po], a, bb;
+                        if (d > 0) { a = L[(d - 1) * HW + po] + P1; if (a < v) v = a; }
+                        if (d < D - 1) { bb = L[(d + 1) * HW + po] + P1; if (bb < v) v = bb; }
+                        if (best + P2 < v) v = best + P2;
+                        L[d * HW + o] = cost[d * HW + o] + v - best;
+                    }
+                }
+                for (d = 0; d < D; d++) agg[d * HW + o] += L[d * HW + o];
+            }
+        }
+    }
+    free(L);
+    return 0;
+}

@@ -62,6 +62,13 @@ def lib() -> C.CDLL:
         L.oracle_consistency.restype = None
         L.oracle_consistency.argtypes = [C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp,
                                          C.c_double, C.c_int, vp]
+        L.oracle_sample_view.restype = None
+        L.oracle_sample_view.argtypes = [C.c_int, C.c_int, C.c_int, vp, vp, vp] + [C.c_double] * 9 + \
+            [C.c_int, C.c_int, vp, vp, vp]
+        L.oracle_box_sat_mean.restype = C.c_int
+        L.oracle_box_sat_mean.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_int, vp]
+        L.oracle_sgm.restype = C.c_int
+        L.oracle_sgm.argtypes = [C.c_int, C.c_int, C.c_int, vp, C.c_float, C.c_float, vp]
         L.oracle_fuse_view.restype = None
         L.oracle_fuse_view.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, C.c_double,
                                        C.c_int, C.c_int, vp, vp, vp]
@@ -343,3 +350,47 @@ def fuse(order, maps, cams, nbrs, rel_tols, px_tol, min_views, point_stride, rgb
     cat = lambda a, shape, dt: np.concatenate(a) if a else np.zeros(shape, dt)
     return (cat(pts, (0, 3), np.float64), cat(cols, (0, 3), np.uint8), cat(nv, (0,), np.uint8),
             cat(owner, (0,), np.int32), {k: u.astype(bool) for k, u in used.items()})
+
+
+# ------------------------------------------------------------------ legacy height sweep (mvs.py)
+def sample_view(img, cam, X0, Y0, gsd, Z):
+    """CPUBackend.sample_view (backend.py:67-76) over _mvs.sample_view (_mvs.pyx:13-58) restated:
+    img (h, w, ch) float32, cam = (R, C, f, k1, k2, k3, cx, cy), Z (H, W) or (D, H, W) heights.
+    Returns (samples (..., H, W, ch) float32, zero where invalid; valid (..., H, W) uint8)."""
+    img = np.ascontiguousarray(img, np.float32)
+    R, Cc, f, k1, k2, k3, cx, cy = cam
+    Z = np.ascontiguousarray(Z, np.float32)
+    h, w, nch = img.shape
+    out = np.zeros(Z.shape + (nch,), np.float32)
+    valid = np.zeros(Z.shape, np.uint8)
+    Zs = Z.reshape((-1,) + Z.shape[-2:])
+    os_ = out.reshape((-1,) + out.shape[-3:])
+    vs = valid.reshape((-1,) + Z.shape[-2:])
+    Rm, Cv = _f64(np.asarray(R, np.float64).reshape(-1)), _f64(np.asarray(Cc, np.float64).reshape(-1))
+    for d in range(Zs.shape[0]):
+        lib().oracle_sample_view(h, w, nch, _p(img), _p(Rm), _p(Cv), float(f), float(k1), float(k2), float(k3),
+                                 float(cx), float(cy), float(X0), float(Y0), float(gsd), Zs.shape[1], Zs.shape[2],
+                                 _p(Zs[d]), _p(os_[d]), _p(vs[d]))
+    return out, valid
+
+
+def box_sat_mean(a, r: int):
+    """_fast.box_sat_mean (_fast.pyx:897-942) restated: (..., H, W) float32 -> window mean."""
+    a = np.ascontiguousarray(a, np.float32)
+    shape = a.shape
+    planes = a.reshape((-1,) + shape[-2:])
+    out = np.empty_like(planes)
+    if lib().oracle_box_sat_mean(planes.shape[0], shape[-2], shape[-1], _p(planes), int(r), _p(out)) != 0:
+        raise ValueError("box_sat_mean: bad radius or out of memory")
+    return out.reshape(shape)
+
+
+def sgm(cost, P1: float, P2: float):
+    """_mvs.sgm (_mvs.pyx:98-251) restated: (D, H, W) float32 cost -> aggregated (D, H, W)."""
+    cost = np.ascontiguousarray(cost, np.float32)
+    D, H, W = cost.shape
+    agg = np.empty_like(cost)
+    if D and H and W:
+        if lib().oracle_sgm(D, H, W, _p(cost), float(P1), float(P2), _p(agg)) != 0:
+            raise MemoryError("sgm")
+    return agg

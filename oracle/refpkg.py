@@ -35,4 +35,16 @@ def load_densify():
         sys.modules["orthomosaic._dense"] = ref._dense
         sys.modules["orthomosaic._fast"] = ref._fast
         sys.modules["orthomosaic._mvs"] = sys.modules["_mvs"]
+        try:
+            import _core  # noqa: F401  (the backend module imports it; built by make -C oracle ref)
+            sys.modules["orthomosaic._core"] = sys.modules["_core"]
+        except ImportError:
+            pass
     return importlib.import_module("orthomosaic.densify")
+
+
+def load_module(name: str):
+    """Another module of the reference package (e.g. "mvs", "backend"), or None."""
+    if load_densify() is None:
+        return None
+    return importlib.import_module(f"orthomosaic.{name}")

@@ -68,6 +68,19 @@ class FuseArgs(C.Structure):
                 ("count", vp)]
 
 
+class SampleViewArgs(C.Structure):
+    _fields_ = [("h", i32), ("w", i32), ("nch", i32), ("img", vp), ("cam", vp), ("X0", C.c_double),
+                ("Y0", C.c_double), ("gsd", C.c_double), ("D", i32), ("H", i32), ("W", i32), ("Z", vp),
+                ("out", vp), ("valid", vp)]
+
+
+class HeightScoreArgs(C.Structure):
+    _fields_ = [("V", i32), ("D", i32), ("H", i32), ("W", i32), ("topk", i32), ("pad_", i32),
+                ("full", C.c_double), ("min_texture", C.c_double), ("full_texture", C.c_double), ("M", vp),
+                ("S2", vp), ("VA", vp), ("PP", vp), ("cxs", vp), ("cys", vp), ("cam_xy", vp), ("score", vp),
+                ("st", vp), ("ref", vp)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("sweep", SweepArgs), ("depth", vp)]
 
@@ -104,6 +117,10 @@ SIGNATURES = {
     "mvs_consistency": (i32, [vp, vp]),
     "mvs_init_normals": (i32, [i32, i32, vp, vp, vp, vp]),
     "mvs_fuse_view": (i32, [vp, vp]),
+    "mvs_sample_view": (i32, [vp, vp]),
+    "mvs_box_sat_mean": (i32, [i32, i32, i32, vp, i32, vp, vp]),
+    "mvs_height_score": (i32, [vp, vp]),
+    "mvs_sgm": (i32, [i32, i32, i32, vp, C.c_float, C.c_float, vp, vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_device_faults": (i32, [vp]),
     "mvs_version": (C.c_char_p, []),

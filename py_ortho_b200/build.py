@@ -25,8 +25,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler",
 EXTRA = {
     "patchmatch.cu": ["-fmad=false"],
     "views.cu": ["-fmad=false"],
+    "height.cu": ["-fmad=false"],
 }
-SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu", "noalloc.cu", "views.cu"]
+SOURCES = ["helpers.cu", "sweep.cu", "patchmatch.cu", "batch.cu", "noalloc.cu", "views.cu", "height.cu"]
 
 
 def nvcc() -> str:

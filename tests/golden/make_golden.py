@@ -25,6 +25,8 @@ Fixtures (each .npz holds the inputs and the reference outputs):
                      depth maps, final filter), recording what the reference's own
                      _consistency, _init_normals and _dense.pm_refine received and returned
   fuse_case.npz    - densify._fuse (point fusion) on views_case's pass-2 maps, in two settings
+  height_case.npz  - the legacy height sweep (mvs.py): _mvs.sample_view, _fast.box_sat_mean and
+                     _mvs.sgm kernel cases, and mvs.dense_reconstruct (CPU backend) end to end
 """
 from __future__ import annotations
 
@@ -473,6 +475,68 @@ def fuse_case(D):
     np.savez_compressed(os.path.join(HERE, "fuse_case.npz"), **res)
 
 
+def height_case(W=160, H=120):
+    """The reference's legacy height sweep (mvs.py) on its CPU backend: kernel cases of
+    _mvs.sample_view (a Z stack into a distorted camera, 3 channels), _fast.box_sat_mean and
+    _mvs.sgm on seeded random inputs, and mvs.dense_reconstruct end to end on a rendered 5-view
+    survey (images through a replaced loader, tie points on the terrain)."""
+    from types import SimpleNamespace
+    from py_ortho_b200 import scene as S
+    M = refpkg.load_module("mvs")
+    B = refpkg.load_module("backend")
+    import _mvs
+    R_ = O.reference()
+    rng = np.random.default_rng(31)
+    res = {}
+    # sample_view
+    img = (rng.random((70, 90, 3)) * 255).astype(np.float32)
+    th = 0.2
+    Rm = np.diag([1.0, -1.0, -1.0]) @ np.array([[np.cos(th), -np.sin(th), 0], [np.sin(th), np.cos(th), 0], [0, 0, 1]])
+    Cc = np.array([2.0, -3.0, 60.0])
+    cam = np.array([80.0, -0.08, 0.02, 0.001, 44.5, 34.5])       # f k1 k2 k3 cx cy
+    Z = (rng.random((4, 50, 60)) * 12 - 2).astype(np.float32)
+    out = np.zeros(Z.shape + (3,), np.float32)
+    val = np.zeros(Z.shape, np.uint8)
+    for d in range(Z.shape[0]):
+        _mvs.sample_view(img, Rm, Cc, *[float(v) for v in cam[:4]], float(cam[4]), float(cam[5]), -25.0, 20.0, 0.7,
+                         Z[d], out[d], val[d])
+    res.update(sv_img=img, sv_R=Rm, sv_C=Cc, sv_cam=cam, sv_grid=np.array([-25.0, 20.0, 0.7]), sv_Z=Z, sv_out=out,
+               sv_valid=val)
+    # box_sat_mean
+    a = (rng.normal(0, 30, (6, 41, 53))).astype(np.float32)
+    res.update(box_in=a, box_r=np.array(3), box_out=R_._fast.box_sat_mean(a, 3))
+    # sgm
+    cost = rng.random((37, 23, 29)).astype(np.float32)
+    res.update(sgm_cost=cost, sgm_p=np.array([0.05, 0.6], np.float32), sgm_out=_mvs.sgm(cost, 0.05, 0.6, 1))
+    # dense_reconstruct on a rendered survey
+    sc = S.make_scene("c1", seed=21, width=W, height=H)
+    cams = [sc.ref_cam] + list(sc.src_cams)
+    imgs = [sc.ref] + list(sc.srcs)
+    X, obs_cam, obs_pt = _tie_points(sc, cams, np.random.default_rng(5), 3000, 30.0, 22.0)
+    intr = [SimpleNamespace(f=float(cams[0].f), cx=float(cams[0].cx), cy=float(cams[0].cy), width=W, height=H,
+                            k1=0.0, k2=0.0, k3=0.0)]
+    rec = SimpleNamespace(used=list(range(len(cams))), intr=intr, cam_group=np.zeros(len(cams), np.int32), X=X,
+                          C=np.array([c.C for c in cams]), R=np.array([c.R for c in cams]))
+    frames = [SimpleNamespace(width=W, height=H, path=f"view{k}") for k in range(len(cams))]
+    ar = SimpleNamespace(frames=frames, backend=B.CPUBackend(), workers=1)
+    rgb = {f"view{k}": np.ascontiguousarray(np.repeat(imgs[k][:, :, None], 3, axis=2)) for k in range(len(cams))}
+    saved = M.load_rgb
+    M.load_rgb = lambda fr, s: rgb[fr.path]
+    try:
+        opt = M.DenseOptions(tile=64, overlap=8, levels=2, workers=1)
+        native = float(sc.ref_cam.C[2] / sc.ref_cam.f)
+        r = M.dense_reconstruct(ar, rec, {}, native, opt)
+    finally:
+        M.load_rgb = saved
+    res.update(h_X=X, h_C=rec.C, h_R=rec.R, h_intr=np.array([intr[0].f, intr[0].cx, intr[0].cy, W, H]),
+               h_native=np.array(native), h_opt=np.array([opt.tile, opt.overlap, opt.levels], np.int64),
+               h_Z=r.Z, h_score=r.score, h_rgb=r.rgb, h_covered=r.covered, h_grid=np.array([r.minX, r.maxY, r.gsd]))
+    for k in range(len(cams)):
+        res[f"h_img{k}"] = imgs[k]
+    print("height_case:", r.Z.shape, float(np.nanmean(r.Z)), float(np.mean(r.score)))
+    np.savez_compressed(os.path.join(HERE, "height_case.npz"), **res)
+
+
 def main():
     D = refpkg.load_densify()
     R = O.reference()
@@ -486,6 +550,7 @@ def main():
     depth_map_case(D)
     views_case(D)
     fuse_case(D)
+    height_case()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -40,7 +40,8 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
     L = _lib()
     structs = {"mvs_hyp": L.Hyp, "mvs_sweep_args": L.SweepArgs, "mvs_pm_args": L.PMArgs,
                "mvs_batch_job": L.BatchJob, "mvs_batch_tuning": L.BatchTuning,
-               "mvs_consistency_args": L.ConsArgs, "mvs_fuse_args": L.FuseArgs}
+               "mvs_consistency_args": L.ConsArgs, "mvs_fuse_args": L.FuseArgs,
+               "mvs_sample_view_args": L.SampleViewArgs, "mvs_height_score_args": L.HeightScoreArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
