@@ -264,7 +264,10 @@ def run_ours(a):
                    "bound": "fp32-issue" if a.pm_precision == "fp32" else "fp64-issue",
                    "evals_per_s": pm_evals / (ms_pm / 1e3),
                    "ms": round(ms_pm, 3), "share_of_step": round(ms_pm / (ms_pm + ms_sweep), 4),
-                   "ncu_profile": PM_PROFILE[a.pm_precision]}
+                   "ncu_profile": PM_PROFILE[a.pm_precision],
+                   "issue_active_ncu": 0.583 if a.pm_precision == "fp32" else 0.667,
+                   "note": "not a contraction and not HBM-bound (DRAM < 1 %): bound by SIMT issue; "
+                           "issue_active is the fraction of SM issue slots used (ncu, see ncu_profile)"}
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
     launches = 2 + (2 * iters if iters else 0)       # sweep + finalize + 2 colour passes per iteration
     line = {

@@ -154,3 +154,24 @@ def test_pm_fp32_refinement_agrees_with_fp64(W, H, n_src, r, step, nan_frac):
           f"within 0.1 % {within:.2%}")
     assert within >= 0.999
     assert 0.8 * cb <= ca <= cb
+
+
+def test_pm_fp32_cost_with_the_geometric_term():
+    """The float32 cost on the reference fixture, whose second source carries a depth map (the
+    geometric term, geo_w 0.5, evaluated in float64 in both modes): with every candidate outside
+    [dmin, dmax] the score map is the current plane's photo term at every pixel."""
+    from py_ortho_b200 import dense
+    z, srcs, sdeps, (r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed) = _case()
+    out = {}
+    for prec in ("fp32", "fp64"):
+        st = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
+        ch = dense.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *st, z["active"], r, step, top_k,
+                             geo_w, geo_tol, 1, 1e9, 1e9 + 1, seed, precision=prec)
+        assert ch == 0
+        out[prec] = st[2].astype(np.float64)
+    a, b = out["fp32"], out["fp64"]
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    d = np.abs(a - b)[np.isfinite(a) & z["active"].astype(bool)]
+    assert d.size > 0
+    assert np.quantile(d, 0.999) <= 1e-5, f"99.9 % quantile {np.quantile(d, 0.999):.2e}"
+    assert d.max() <= 1e-3, f"max {d.max():.2e}"
