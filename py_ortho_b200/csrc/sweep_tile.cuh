@@ -487,6 +487,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
     float* sW = reinterpret_cast<float*>(sH + HR * TW);
     Coef* sC = reinterpret_cast<Coef*>(sW + 6 * TH * TW);
     const int c = tid % TW, seg = tid / TW;
+    const float fcol = (float)c, fseg = (float)seg;
     const int gx = tx + c;
     float mu[ROWS], rsd[ROWS];
     const bool to_rec = chunk >= 0;
@@ -546,24 +547,42 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                 const Coef cf = sC[s];
                 constexpr int PER = (HR * HC + NT - 1) / NT;
                 if (WIDE && cf.inside && tile_inside) {
-                    // every sample of the thread gathered before any is stored (the surplus of the
-                    // last round repeats the tile's last sample and is not stored): the gathers
-                    // are independent and in flight together
-                    float Jv[PER];
-                    int off[PER];
+                    // every sample of the thread gathered before any is stored: the gathers are
+                    // independent and in flight together. The thread keeps halo column c and
+                    // rows seg, seg + SEG, ... (positions and shared offsets fixed per thread, so
+                    // no per-sample index arithmetic); the 2R right-hand halo columns are spread
+                    // over all threads. A surplus row repeats the last row and is not stored.
+                    constexpr int MR = (HR + SEG - 1) / SEG;
+                    constexpr int XW = R > 0 ? 2 * R : 1, XS = 2 * R * HR, PX = (XS + NT - 1) / NT;
+                    float Jv[MR + PX];
 #pragma unroll
-                    for (int k = 0; k < PER; ++k) {
-                        const int e0 = tid + k * NT;
-                        const int e = e0 < HR * HC ? e0 : HR * HC - 1;
-                        const int hy = e / HC, hc = e - hy * HC;
-                        Jv[k] = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
-                        off[k] = e0 < HR * HC ? hy * JP + (RA - R) + hc : -1;
+                    for (int k = 0; k < MR; ++k) {
+                        const float b = (k + 1) * SEG > HR ? fminf(fseg + (float)(k * SEG), (float)(HR - 1))
+                                                           : fseg + (float)(k * SEG);
+                        Jv[k] = sample_plane_inside<F16>(cf, img, sw, sh, fcol, b);
                     }
 #pragma unroll
-                    for (int k = 0; k < PER; ++k) {
-                        if (off[k] >= 0) {
+                    for (int m = 0; m < PX; ++m) {
+                        const int e0 = tid + m * NT;
+                        const int e = e0 < XS ? e0 : XS - 1;
+                        const int hy = e / XW, hc = TW + (e - hy * XW);
+                        Jv[MR + m] = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
+                    }
+                    float* col = sJ + seg * JP + (RA - R) + c;
+#pragma unroll
+                    for (int k = 0; k < MR; ++k) {
+                        if ((k + 1) * SEG <= HR || seg + k * SEG < HR) {
                             any_invalid |= Jv[k] != Jv[k];
-                            sJ[off[k]] = Jv[k];
+                            col[k * SEG * JP] = Jv[k];
+                        }
+                    }
+#pragma unroll
+                    for (int m = 0; m < PX; ++m) {
+                        const int e0 = tid + m * NT;
+                        if (e0 < XS) {
+                            const int hy = e0 / XW, hc = TW + (e0 - hy * XW);
+                            any_invalid |= Jv[MR + m] != Jv[MR + m];
+                            sJ[hy * JP + (RA - R) + hc] = Jv[MR + m];
                         }
                     }
                 } else if (cf.inside && tile_inside) {
