@@ -68,9 +68,13 @@ typedef struct mvs_hyp {
 
 /* Storage precision of source images and warped tiles. */
 typedef enum mvs_precision {
-    MVS_PREC_FP32 = 0,   /* plain: float32 images and tiles, FP32 window sums                      */
-    MVS_PREC_FP16 = 1    /* FP16 images (src pointers are __half) and FP16 warped tiles; FP32 sums
-                            with compensated variance terms; FP64 homography and parabola          */
+    MVS_PREC_FP32 = 0,      /* plain: float32 images and tiles, FP32 window sums                   */
+    MVS_PREC_FP16 = 1,      /* FP16 images (src pointers are __half), FP32 window sums; PLANES only;
+                               FP64 homography and parabola                                        */
+    MVS_PREC_FP64_SUMS = 2  /* float32 images and tiles, window sums in float64 as the reference
+                               keeps them (_sweep.h:85-178): its NCC to ~1 float32 ulp even on
+                               bright low-texture windows, where FP32 sums differ by up to ~1e-3;
+                               single-view calls (mvs_sweep*) only, slower stages B and C        */
 } mvs_precision;
 
 typedef struct mvs_sweep_args {

@@ -23,7 +23,7 @@ MAX_PLANES_PER_CALL = 1024
 
 OK, ERR_VALUE, ERR_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(6)
 HYP_MAPS, HYP_LINEAR, HYP_REFINE, HYP_PLANES = range(4)
-PREC_FP32, PREC_FP16 = 0, 1
+PREC_FP32, PREC_FP16, PREC_FP64_SUMS = 0, 1, 2
 
 vp = C.c_void_p
 i32 = C.c_int32

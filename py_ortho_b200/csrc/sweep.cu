@@ -40,12 +40,12 @@ static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r) 
     return e == CUDA_SUCCESS;
 }
 
-template <int R, int KMAX, bool PLANES, bool F16>
+template <int R, int KMAX, bool PLANES, bool F16, bool X64>
 __global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ SweepParams p) {
     extern __shared__ __align__(128) float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, KMAX, PLANES, F16, true, true>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
+    sweep_tile<R, KMAX, PLANES, F16, true, true, X64>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
                                                  p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
 }
 
@@ -93,9 +93,9 @@ __global__ void finalize_kernel(int H, int W, int kind, int n, int t0, const flo
 
 // ------------------------------------------------------------------------------ launcher
 
-template <int R, int KMAX, bool PLANES, bool F16>
+template <int R, int KMAX, bool PLANES, bool F16, bool X64>
 static mvs_status launch_sweep(const SweepParams& p, dim3 grid, cudaStream_t st) {
-    auto kern = sweep_kernel<R, KMAX, PLANES, F16>;
+    auto kern = sweep_kernel<R, KMAX, PLANES, F16, X64>;
     const size_t smem = Geom<R>::smem_bytes();
     // the attribute is per function and per device: set it for the current device every time
     MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
@@ -104,23 +104,28 @@ static mvs_status launch_sweep(const SweepParams& p, dim3 grid, cudaStream_t st)
     return check_launch("sweep kernel");
 }
 
-template <int KMAX, bool PLANES, bool F16>
+template <int KMAX, bool PLANES, bool F16, bool X64 = false>
 static mvs_status dispatch_r(int r, const SweepParams& p, dim3 grid, cudaStream_t st) {
     switch (r) {
-        case 0: return launch_sweep<0, KMAX, PLANES, F16>(p, grid, st);
-        case 1: return launch_sweep<1, KMAX, PLANES, F16>(p, grid, st);
-        case 2: return launch_sweep<2, KMAX, PLANES, F16>(p, grid, st);
-        case 3: return launch_sweep<3, KMAX, PLANES, F16>(p, grid, st);
-        case 4: return launch_sweep<4, KMAX, PLANES, F16>(p, grid, st);
-        case 5: return launch_sweep<5, KMAX, PLANES, F16>(p, grid, st);
-        case 6: return launch_sweep<6, KMAX, PLANES, F16>(p, grid, st);
-        case 7: return launch_sweep<7, KMAX, PLANES, F16>(p, grid, st);
+        case 0: return launch_sweep<0, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 1: return launch_sweep<1, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 2: return launch_sweep<2, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 3: return launch_sweep<3, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 4: return launch_sweep<4, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 5: return launch_sweep<5, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 6: return launch_sweep<6, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 7: return launch_sweep<7, KMAX, PLANES, F16, X64>(p, grid, st);
     }
     return fail(MVS_ERR_VALUE, "sweep: window radius %d outside 0..%d", r, MVS_MAX_RADIUS);
 }
 
-static mvs_status dispatch(int r, int kmax, bool planes, bool f16, const SweepParams& p, dim3 grid,
+static mvs_status dispatch(int r, int kmax, bool planes, bool f16, bool x64, const SweepParams& p, dim3 grid,
                            cudaStream_t st) {
+    if (x64) {
+        if (planes) return kmax <= 2 ? dispatch_r<2, true, false, true>(r, p, grid, st)
+                                     : dispatch_r<8, true, false, true>(r, p, grid, st);
+        return kmax <= 2 ? dispatch_r<2, false, false, true>(r, p, grid, st) : dispatch_r<8, false, false, true>(r, p, grid, st);
+    }
     if (planes) {
         if (f16) return kmax <= 2 ? dispatch_r<2, true, true>(r, p, grid, st) : dispatch_r<8, true, true>(r, p, grid, st);
         return kmax <= 2 ? dispatch_r<2, true, false>(r, p, grid, st) : dispatch_r<8, true, false>(r, p, grid, st);
@@ -144,7 +149,8 @@ mvs_status validate_sweep(const mvs_sweep_args* a) {
     if (a->top_k < 1) return fail(MVS_ERR_VALUE, "sweep: top_k must be >= 1");
     if (!a->geo) return fail(MVS_ERR_VALUE, "geo must be (n_sources, 18)");
     if (a->i1 < a->i0) return fail(MVS_ERR_VALUE, "sweep: empty or reversed hypothesis range");
-    if (a->precision != MVS_PREC_FP32 && a->precision != MVS_PREC_FP16) return fail(MVS_ERR_VALUE, "sweep: unknown precision");
+    if (a->precision != MVS_PREC_FP32 && a->precision != MVS_PREC_FP16 && a->precision != MVS_PREC_FP64_SUMS)
+        return fail(MVS_ERR_VALUE, "sweep: unknown precision");
     const int kind = a->hyp.kind;
     if (kind < MVS_HYP_MAPS || kind > MVS_HYP_PLANES) return fail(MVS_ERR_VALUE, "sweep: unknown hypothesis kind");
     if (a->H == 0 || a->W == 0) return MVS_OK;
@@ -261,7 +267,8 @@ mvs_status sweep_range(const mvs_sweep_args* a, int i0, int i1, float* rec_ws, i
     p.nchunks = used;
     p.r = a->r;
     dim3 grid((a->W + TW - 1) / TW, (a->H + TH - 1) / TH, used);
-    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision == MVS_PREC_FP16, p, grid, st));
+    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision == MVS_PREC_FP16,
+                     a->precision == MVS_PREC_FP64_SUMS, p, grid, st));
     if (used > 1) {
         const long long HW = (long long)a->H * a->W;
         merge_kernel<<<(unsigned)((HW + 255) / 256), 256, 0, st>>>(HW, used, i0, i1, p.ppc, rec_ws, a->best, a->prev,

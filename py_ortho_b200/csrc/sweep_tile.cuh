@@ -400,6 +400,121 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
     }
 }
 
+// ---- float64 window sums (MVS_PREC_FP64_SUMS): the reference's arithmetic for the sums
+// (_sweep.h:85-178): horizontal window sums of J, J^2 and J I accumulated in float64 (products of
+// float32 values are exact there) and stored rounded to float32, as the reference stores its hs
+// rows; vertical sums, moments, variance and NCC in float64, the NCC rounded to float32 once.
+// On bright low-texture windows, where the NCC divides by sd_ref * sd_src ~ 1e-3, float32 running
+// sums differ from the reference by up to ~1e-3; these track it to the last float32 bit or so.
+
+template <int R, bool WITHV>
+__device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, float4* sH, int tid) {
+    using G = Geom<R>;
+    constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
+    if (tid >= HR * NSEG) return;
+    const int sg = tid / HR, hy = tid - sg * HR;
+    const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
+    const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
+    float v[NIN], jz[NIN], iz[NIN];
+#pragma unroll
+    for (int q = 0; q < NIN / 4; ++q) {
+        const float4 a = jr[q], b = ir[q];
+        const float jv[4] = {a.x, a.y, a.z, a.w}, iv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = 4 * q + u;
+            float x = jv[u];
+            if constexpr (WITHV) {
+                const bool ok = x == x;
+                x = ok ? x : 0.f;
+                v[t] = ok ? 1.f : 0.f;
+            }
+            jz[t] = x;
+            iz[t] = iv[u];
+        }
+    }
+    float a0 = 0.f;                       // counts are small integers: exact in float32
+    double a1 = 0.0, a2 = 0.0, a3 = 0.0;
+#pragma unroll
+    for (int t = RA - R; t <= RA + R; ++t) {
+        if constexpr (WITHV) a0 = __fadd_rn(a0, v[t]);
+        const double j = jz[t];
+        a1 = __dadd_rn(a1, j);
+        a2 = __fma_rn(j, j, a2);
+        a3 = __fma_rn(j, (double)iz[t], a3);
+    }
+    float4* row = sH + hy * TW + P * sg;
+    const int kx = (sg + hy) & 7;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        if (j > 0) {
+            const int tn = RA + R + j, to = RA - R + j - 1;
+            if constexpr (WITHV) a0 = __fadd_rn(a0, __fsub_rn(v[tn], v[to]));
+            const double jn = jz[tn], jo = jz[to];
+            a1 = __dsub_rn(__dadd_rn(a1, jn), jo);
+            a2 = __fma_rn(-jo, jo, __fma_rn(jn, jn, a2));
+            a3 = __fma_rn(-jo, (double)iz[to], __fma_rn(jn, (double)iz[tn], a3));
+        }
+        row[j ^ kx] = make_float4(a0, (float)a1, (float)a2, (float)a3);
+    }
+}
+
+// `sdv` holds the reference's window deviation itself (not its reciprocal) in this mode.
+template <int R, int KMAX, bool WITHV>
+__device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const float* mu, const float* sdv,
+                                          float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
+    constexpr int K = 2 * R + 1;
+    const float k2 = (float)(K * K);
+    static_assert(ROWS % 8 == 0, "stage C rows must start on a multiple of 8");
+    int sw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
+    const float4* col = sH + y0 * TW;
+    float cv = 0.f;
+    double cj = 0.0, cjj = 0.0, cji = 0.0;
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+        const float4 h = col[t * TW + sw[t & 7]];
+        if constexpr (WITHV) cv = __fadd_rn(cv, h.x);
+        cj = __dadd_rn(cj, (double)h.y);
+        cjj = __dadd_rn(cjj, (double)h.z);
+        cji = __dadd_rn(cji, (double)h.w);
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        if (j > 0) {
+            const float4 hn = col[(j + 2 * R) * TW + sw[(j + 2 * R) & 7]];
+            const float4 ho = col[(j - 1) * TW + sw[(j - 1) & 7]];
+            if constexpr (WITHV) cv = __fadd_rn(cv, __fsub_rn(hn.x, ho.x));
+            cj = __dsub_rn(__dadd_rn(cj, (double)hn.y), (double)ho.y);
+            cjj = __dsub_rn(__dadd_rn(cjj, (double)hn.z), (double)ho.z);
+            cji = __dsub_rn(__dadd_rn(cji, (double)hn.w), (double)ho.w);
+        }
+        float ncc;
+        if (WITHV && cv * 10.f <= 9.f * k2) {
+            ncc = -1.f;
+        } else {
+            const double n = WITHV ? (double)cv : (double)k2;
+            const double mj = __ddiv_rn(cj, n), m2 = __ddiv_rn(cjj, n), mij = __ddiv_rn(cji, n);
+            const double var = __dsub_rn(m2, __dmul_rn(mj, mj));
+            const double sdj = var > 1e-6 ? __dsqrt_rn(var) : 1e-3;
+            double x = __ddiv_rn(__dsub_rn(mij, __dmul_rn((double)mu[j], mj)), __dmul_rn((double)sdv[j], sdj));
+            x = x > 1.0 ? 1.0 : (x < -1.0 ? -1.0 : x);
+            ncc = (float)x;
+        }
+        if (bottom) total[j] = __fadd_rn(total[j], ncc);
+        float x = ncc;
+#pragma unroll
+        for (int q = 0; q < KMAX; ++q) {
+            if (q < nlist) {
+                const float hi = fmaxf(topk[j][q], x), lo = fminf(topk[j][q], x);
+                topk[j][q] = bottom ? lo : hi;
+                x = bottom ? hi : lo;
+            }
+        }
+    }
+}
+
 // ---- the reference tile by TMA (single-view kernel): one 2D tiled bulk copy per CTA, completed
 // on an mbarrier. The copy's box is the tile with its halo, JP x HR floats starting at
 // (tx - RA, ty - R): x is a multiple of 4 floats (16 bytes), rows outside the image read as 0,
@@ -450,7 +565,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // flight; more registers - the single-view kernel, whose radius is a template argument, uses it).
 // REF_TMA: the reference tile arrives by TMA when p.ref_tma is set (the single-view kernel, whose
 // parameters hold the tensor map; `smem` must then be 128-byte aligned).
-template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false>
+template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false, bool X64 = false>
 __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
     using G = Geom<R>;
     constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
@@ -497,7 +612,8 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
         const bool in = gx < W && gy < H;
         const long long o = (long long)gy * W + gx;
         mu[j] = in ? __ldg(p.mu + o) : 0.f;
-        rsd[j] = in ? 1.0f / __ldg(p.sd + o) : 0.f;
+        // X64: the deviation itself (stage C divides in float64); else its reciprocal
+        rsd[j] = in ? (X64 ? __ldg(p.sd + o) : 1.0f / __ldg(p.sd + o)) : 0.f;
         const bool load = in && !to_rec && !p.fresh;
         const int w = ly * TW + c;
         sW[w] = load ? p.best[o] : -2.f;
@@ -625,14 +741,26 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             const bool all_valid = !__syncthreads_or(any_invalid);
             // ---- B: horizontal window sums of (V, J, J^2, J I), one 16-column row segment per
             // thread: products once per input, running sums along the segment
-            if (all_valid) {
+            if constexpr (X64) {
+                if (all_valid) {
+                    stage_b64<R, false>(sJ, sI, sH, tid);
+                } else {
+                    stage_b64<R, true>(sJ, sI, sH, tid);
+                }
+            } else if (all_valid) {
                 stage_b<R, false>(sJ, sI, sH, tid);
             } else {
                 stage_b<R, true>(sJ, sI, sH, tid);
             }
             __syncthreads();
             // ---- C: vertical running sums down the column, NCC, top-k insertion
-            if (all_valid) {
+            if constexpr (X64) {
+                if (all_valid) {
+                    stage_c64<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                } else {
+                    stage_c64<R, KMAX, true>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                }
+            } else if (all_valid) {
                 stage_c<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
             } else {
                 stage_c<R, KMAX, true>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);

@@ -43,7 +43,8 @@ class DepthOptions:
     point_stride: int = 2
     cache_mb: int = 1200
     workers: int = 0
-    precision: int = L.PREC_FP32      # FP16 storage of source images (constant-plane sweeps only)
+    precision: int = L.PREC_FP32      # PREC_FP16: FP16 source storage (constant-plane sweeps only);
+    #                                   PREC_FP64_SUMS: window sums in float64 as the reference keeps them
     pm_precision: str = "fp64"        # PatchMatch cost: "fp64" (the reference's arithmetic) or "fp32"
 
 
@@ -269,6 +270,12 @@ def _upsample2(a: torch.Tensor, H: int, W: int) -> torch.Tensor:
     return up.contiguous()
 
 
+def _per_pixel_precision(opt) -> int:
+    """Sweeps over per-pixel hypothesis maps read float32 images; only the float64-sums mode
+    carries over from the options (FP16 storage needs constant planes)."""
+    return L.PREC_FP64_SUMS if opt.precision == L.PREC_FP64_SUMS else L.PREC_FP32
+
+
 def depth_map(k, nbrs, rec, views, opt: DepthOptions):
     """Depth (camera-axis, metres) and NCC score for reference image `k` at matching scale, with the
     reference's coarse-to-fine schedule (densify.py:373-437): full sweep at 1/4 resolution over a
@@ -312,7 +319,7 @@ def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
     step = ((inv_hi - inv_lo) / max(nd - 1, 1)).astype(np.float32)
     base_t, step_t = _dev(inv_lo), _dev(step)
     d, _, _, _ = sweep_device(pyr_r[lv], pyr_c[lv], pyr_s[lv], pyr_cs[lv], Hypotheses.linear(base_t, step_t, nd),
-                              opt, rays[lv], precision=L.PREC_FP32)
+                              opt, rays[lv], precision=_per_pixel_precision(opt))
     dstep = step_t / 2
     score = sd = None
     for lvl in range(lv - 1, -1, -1):
@@ -322,7 +329,7 @@ def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
         iu = (1.0 / up).contiguous()
         d, score, sd, _ = sweep_device(pyr_r[lvl], pyr_c[lvl], pyr_s[lvl], pyr_cs[lvl],
                                        Hypotheses.refine(iu, dstep, opt.refine_steps), opt, rays[lvl],
-                                       precision=L.PREC_FP32)
+                                       precision=_per_pixel_precision(opt))
         dstep = dstep / 2
     mask = torch.from_numpy(ref_mask).to(d.device)
     depth = torch.where(mask | (d < rng[0]) | (d > rng[1]), torch.full_like(d, float("nan")), d)

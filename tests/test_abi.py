@@ -94,6 +94,27 @@ def test_validation_errors_need_no_device():
     p.S = 17
     assert lib.mvs_pm_refine(ctypes.addressof(p), None) == L.OK
     assert lib.mvs_batch_create(None, 0, None, ctypes.byref(ctypes.c_void_p())) == L.ERR_VALUE
+    # precision modes: an unknown one is refused; float64 window sums are single-view only
+    b = L.SweepArgs()
+    b.n_src, b.r, b.top_k, b.geo, b.precision = 1, 1, 1, geo.ctypes.data, 3
+    assert lib.mvs_sweep(ctypes.addressof(b), None) == L.ERR_VALUE
+    assert "unknown precision" in L.last_error()
+    h = ctypes.c_void_p()
+    assert lib.mvs_server_create(4, 4, 3, L.PREC_FP64_SUMS, ctypes.byref(h)) == L.ERR_UNSUPPORTED
+    assert "single-view" in L.last_error()
+
+
+def test_precision_values_match_the_header(tmp_path):
+    L = _lib()
+    names = {"MVS_PREC_FP32": L.PREC_FP32, "MVS_PREC_FP16": L.PREC_FP16, "MVS_PREC_FP64_SUMS": L.PREC_FP64_SUMS}
+    src = ['#include <stdio.h>', f'#include "{HEADER}"', "int main(void) {"]
+    src += [f'printf("{n} %d\\n", (int){n});' for n in names] + ["return 0; }"]
+    c = tmp_path / "enums.c"
+    c.write_text("\n".join(src))
+    exe = tmp_path / "enums"
+    subprocess.run(["gcc", "-std=c11", "-o", str(exe), str(c)], check=True)
+    out = dict(l.split() for l in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    assert {k: int(v) for k, v in out.items()} == names
 
 
 def test_python_layer_validates_before_touching_the_device():
