@@ -23,7 +23,10 @@
 //      insertion into a per-pixel top-k list in registers.
 // After the last source the winner-take-all state of each pixel is updated in registers; it
 // leaves the SM once per hypothesis chunk. Window sums are short FP32 sums (at most TH/SEG
-// add/subtract steps), so the reference's float64 running sums are not needed.
+// add/subtract steps): within the parity bar wherever the window has texture, but on bright
+// low-texture windows at r <= 2 their rounding, amplified by 1 / (sd_ref sd_src), can reach
+// ~1e-3 in NCC. X64 (MVS_PREC_FP64_SUMS) keeps the sums in float64 as the reference does
+// (stage_b64 / stage_c64).
 #pragma once
 
 #include "common.cuh"
