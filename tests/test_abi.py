@@ -102,6 +102,23 @@ def test_validation_errors_need_no_device():
     h = ctypes.c_void_p()
     assert lib.mvs_server_create(4, 4, 3, L.PREC_FP64_SUMS, ctypes.byref(h)) == L.ERR_UNSUPPORTED
     assert "single-view" in L.last_error()
+    jobs = (L.BatchJob * 1)()
+    j = jobs[0].sweep
+    j.n_src, j.r, j.top_k, j.geo, j.precision = 1, 1, 1, geo.ctypes.data, L.PREC_FP64_SUMS
+    j.hyp.kind = L.HYP_PLANES
+    assert lib.mvs_batch_create(ctypes.addressof(jobs), 1, None, ctypes.byref(h)) == L.ERR_UNSUPPORTED
+    assert "single-view" in L.last_error()
+
+
+def test_depth_map_keeps_only_the_float64_sums_mode_on_per_pixel_sweeps():
+    from py_ortho_b200 import densify
+    L = _lib()
+    opt = densify.DepthOptions()
+    assert densify._per_pixel_precision(opt) == L.PREC_FP32
+    opt.precision = L.PREC_FP16              # FP16 storage needs constant planes
+    assert densify._per_pixel_precision(opt) == L.PREC_FP32
+    opt.precision = L.PREC_FP64_SUMS
+    assert densify._per_pixel_precision(opt) == L.PREC_FP64_SUMS
 
 
 def test_precision_values_match_the_header(tmp_path):
