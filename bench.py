@@ -268,8 +268,14 @@ def run_ours(a):
                    "issue_active_ncu": 0.583 if a.pm_precision == "fp32" else 0.667,
                    "note": "not a contraction and not HBM-bound (DRAM < 1 %): bound by SIMT issue; "
                            "issue_active is the fraction of SM issue slots used (ncu, see ncu_profile)"}
+    L.check_device_faults()        # a sweep tile that gave up its bounded wait makes the run fail
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
-    launches = 2 + (2 * iters if iters else 0)       # sweep + finalize + 2 colour passes per iteration
+    # our kernels per step: the sweep (+ the ordered chunk merge when its planes are split over
+    # CTAs: mvs_sweep's automatic rule, tiles below 6 CTAs per SM), finalize, and per PatchMatch
+    # call the stream start plus, per colour pass, propagation, count, scan, stream states, trials
+    tiles = ((W + 63) // 64) * ((H + 31) // 32)
+    sweep_launches = 1 if tiles >= 6 * torch.cuda.get_device_properties(dev).multi_processor_count else 2
+    launches = sweep_launches + 1 + ((1 + 10 * iters) if iters else 0)
     line = {
         "metric": "ZNCC evaluations/s (pixel x plane x view), sweep + PatchMatch",
         "value": value / 1e9, "unit": "Gpix.plane.view/s", "n_gpus": world, "steps": a.steps,
@@ -292,7 +298,7 @@ def run_ours(a):
         line["e2e"] = run_e2e(a, ref_h, srcs_h, geo, ref_cam, hyp, r, top_k, pm, normal0, H, W, iters, evals, world,
                               prec)
     if rank == 0 and not a.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(cfg, nplanes, iters, budget_s=12.0)
+        line["cpu_baseline"] = cpu_baseline(cfg, nplanes, iters, device=dev)   # sample rendered on the GPU
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -397,110 +403,132 @@ def read_traffic(kernel: str):
 
 
 # ------------------------------------------------------------------ CPU baseline (reference code)
-def cpu_baseline(cfg, nplanes, iters, budget_s: float = 12.0):
+class CpuSample:
     """The reference's own CPU kernels (oracle/_ref: _dense.sweep_hypothesis and _dense.pm_refine
-    compiled from its sources; falls back to the oracle's C restatement when the reference was
-    not built) timed on a bounded sample of the same workload with a thread pool over all host
-    cores (row bands of the view, as densify's view-level thread pool keeps every core busy).
-    Throughput in the same unit; the full-size step time is extrapolated per evaluation."""
-    from concurrent.futures import ThreadPoolExecutor
-    from oracle import oracle as O
-    from py_ortho_b200 import scene as S
-    R = O.reference()
-    kind = "reference" if R is not None else "port"
-    cores = os.cpu_count() or 1
-    r = cfg.radius
-    # sample: a reduced-size view with the workload's source count, window and plane spacing
-    sc = S.make_scene(cfg, seed=0, width=512, height=384)
-    ref = sc.grey(sc.ref)
-    srcs = [sc.grey(s) for s in sc.srcs]
-    H, W = ref.shape
-    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
-    ray = O.rays_world((H, W), sc.ref_cam)
-    planes = S.plane_list(cfg.depth_range[0], cfg.depth_range[1], nplanes)
-    mu, sd = O.ref_stats(ref, r)
-    nb = cores
-    bands = [(max(0, (H * k) // nb - r), min(H, (H * (k + 1)) // nb + r), (H * k) // nb, (H * (k + 1)) // nb)
-             for k in range(nb)]
-    n_pl = max(1, min(nplanes, 32))
-    sel = planes[np.linspace(0, nplanes - 1, n_pl).astype(int)]
+    compiled from its sources; the oracle's C restatement when the reference was not built) on a
+    bounded sample of the benchmark's workload, with a thread pool over all host cores (row bands
+    of the view, as densify's view-level thread pool keeps every core busy). The sample view is
+    rendered once; measure() times one pass over it (about 2 s on 16 cores) and extrapolates the
+    full step per evaluation, in the benchmark's unit.
 
-    def band(b):
-        y0, y1, _, _ = b
-        st = O.init_state(y1 - y0, W)
-        rr, mm, ss, ry = (np.ascontiguousarray(x[..., y0:y1, :]) for x in (ref, mu, sd, ray))
-        for i, p in enumerate(sel):
-            inv = np.full((y1 - y0, W), p, np.float32)
-            if R is not None:
-                R._dense.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
-            else:
-                O.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
-        return (b[3] - b[2]) * W * len(sel) * len(srcs)
+    Sample: a 512 x 384 view of the same scene family with the workload's sources, window and all
+    of its planes (the same plane spacing); PatchMatch: 4 cores' worth of 64 x 48 crops per core,
+    one iteration each, starting from the scene's true depth (the GPU arm starts from the sweep's
+    depth and runs 4 iterations; a pixel-iteration costs the same candidate evaluations either
+    way). The metric counts a PatchMatch pixel-iteration as 11 candidate evaluations x sources."""
 
-    t0 = time.perf_counter()
-    with ThreadPoolExecutor(cores) as ex:
-        sweep_done = sum(ex.map(band, bands))
-    t_sweep = time.perf_counter() - t0
-    sweep_rate = sweep_done / t_sweep
-    pm_rate = None
-    if iters and R is not None:
-        ph, pw = 48, 64
-        crops = []
-        for k in range(cores):
-            y0 = (k * 37) % (H - ph)
-            x0 = (k * 53) % (W - pw)
-            crops.append((y0, x0))
-        par = np.array([c.row() for c in sc.src_cams], np.float64)
+    def __init__(self, cfg, nplanes, iters, device="cpu"):
+        from oracle import oracle as O
+        from py_ortho_b200 import scene as S
+        self.O, self.R = O, O.reference()
+        self.cfg, self.nplanes, self.iters = cfg, nplanes, iters
+        self.kind = "reference" if self.R is not None else "port"
+        self.cores = os.cpu_count() or 1
+        sc = S.make_scene(cfg, seed=0, width=512, height=384, device=device)
+        self.sc = sc
+        self.ref = sc.grey(sc.ref)
+        self.srcs = [sc.grey(s) for s in sc.srcs]
+        H, W = self.ref.shape
+        self.geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+        self.ray = O.rays_world((H, W), sc.ref_cam)
+        self.planes = S.plane_list(cfg.depth_range[0], cfg.depth_range[1], nplanes)
+        self.mu, self.sd = O.ref_stats(self.ref, cfg.radius)
+        self.par = np.array([c.row() for c in sc.src_cams], np.float64)
+        self.normals = S.tilted_normals(48, 64, 7)
 
-        def pm_crop(c):
-            y0, x0 = c
-            rr = np.ascontiguousarray(ref[y0:y0 + ph, x0:x0 + pw])
-            ry = np.ascontiguousarray(ray[:, y0:y0 + ph, x0:x0 + pw])
-            d = np.ascontiguousarray(sc.depth_true[y0:y0 + ph, x0:x0 + pw], np.float32)
-            nrm = S.tilted_normals(ph, pw, 7)
-            scr = np.zeros((ph, pw), np.float32)
-            act = np.ones((ph, pw), np.uint8)
-            R._dense.pm_refine(rr, ry, np.asarray(sc.ref_cam.C, np.float64), srcs, [None] * len(srcs), par, d, nrm,
-                               scr, act, cfg.pm_radius, cfg.pm_step, cfg.top_k, 0.5, 0.02, 1, cfg.depth_range[0],
-                               cfg.depth_range[1], 7)
-            return ph * pw * PM_HYPS * len(srcs)
+    def measure(self):
+        from concurrent.futures import ThreadPoolExecutor
+        O, R, cfg = self.O, self.R, self.cfg
+        r, cores = cfg.radius, self.cores
+        ref, srcs, ray, geo, mu, sd = self.ref, self.srcs, self.ray, self.geo, self.mu, self.sd
+        H, W = ref.shape
+        bands = [(max(0, (H * k) // cores - r), min(H, (H * (k + 1)) // cores + r), (H * k) // cores,
+                  (H * (k + 1)) // cores) for k in range(cores)]
+
+        def band(b):
+            y0, y1, _, _ = b
+            st = O.init_state(y1 - y0, W)
+            rr, mm, ss, ry = (np.ascontiguousarray(x[..., y0:y1, :]) for x in (ref, mu, sd, ray))
+            for i, p in enumerate(self.planes):
+                inv = np.full((y1 - y0, W), p, np.float32)
+                if R is not None:
+                    R._dense.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
+                else:
+                    O.sweep_hypothesis(rr, mm, ss, srcs, ry, geo, inv, r, cfg.top_k, i, *st)
+            return (b[3] - b[2]) * W * len(self.planes) * len(srcs)
 
         t0 = time.perf_counter()
         with ThreadPoolExecutor(cores) as ex:
-            pm_done = sum(ex.map(pm_crop, crops))
-        pm_rate = pm_done / (time.perf_counter() - t0)
-    full_sweep = cfg.width * cfg.height * nplanes * len(srcs)
-    full_pm = cfg.width * cfg.height * iters * PM_HYPS * len(srcs)
-    t_full = full_sweep / sweep_rate + (full_pm / pm_rate if pm_rate else 0.0)
-    return {"value": (full_sweep + full_pm) / t_full / 1e9, "unit": "Gpix.plane.view/s", "cores": cores,
-            "kind": kind, "sweep_rate": sweep_rate / 1e9, "pm_rate": None if pm_rate is None else pm_rate / 1e9,
-            "sample": f"sweep: 512x384 view, {len(srcs)} sources, {len(sel)} of {nplanes} planes, "
-                      f"{len(bands)} row bands on {cores} threads; PatchMatch: {cores} 64x48 crops x 1 iteration; "
-                      f"full step extrapolated per evaluation ({t_full:.1f} s)"}
+            sweep_done = sum(ex.map(band, bands))
+        sweep_rate = sweep_done / (time.perf_counter() - t0)
+        pm_rate = None
+        ncrop = 4 * cores
+        if self.iters and R is not None:
+            ph, pw = 48, 64
+            crops = [((k * 37) % (H - ph), (k * 53) % (W - pw)) for k in range(ncrop)]
+            sc = self.sc
+
+            def pm_crop(c):
+                y0, x0 = c
+                rr = np.ascontiguousarray(ref[y0:y0 + ph, x0:x0 + pw])
+                ry = np.ascontiguousarray(ray[:, y0:y0 + ph, x0:x0 + pw])
+                d = np.ascontiguousarray(sc.depth_true[y0:y0 + ph, x0:x0 + pw], np.float32)
+                nrm = self.normals.copy()
+                scr = np.zeros((ph, pw), np.float32)
+                act = np.ones((ph, pw), np.uint8)
+                R._dense.pm_refine(rr, ry, np.asarray(sc.ref_cam.C, np.float64), srcs, [None] * len(srcs), self.par,
+                                   d, nrm, scr, act, cfg.pm_radius, cfg.pm_step, cfg.top_k, 0.5, 0.02, 1,
+                                   cfg.depth_range[0], cfg.depth_range[1], 7)
+                return ph * pw * PM_HYPS * len(srcs)
+
+            t0 = time.perf_counter()
+            with ThreadPoolExecutor(cores) as ex:
+                pm_done = sum(ex.map(pm_crop, crops))
+            pm_rate = pm_done / (time.perf_counter() - t0)
+        full_sweep = cfg.width * cfg.height * self.nplanes * len(srcs)
+        full_pm = cfg.width * cfg.height * self.iters * PM_HYPS * len(srcs)
+        t_full = full_sweep / sweep_rate + (full_pm / pm_rate if pm_rate else 0.0)
+        return {"value": (full_sweep + full_pm) / t_full / 1e9, "unit": "Gpix.plane.view/s", "cores": cores,
+                "kind": self.kind, "sweep_rate": sweep_rate / 1e9,
+                "pm_rate": None if pm_rate is None else pm_rate / 1e9, "step_s_extrapolated": t_full,
+                "sample": f"sweep: 512x384 view, {len(srcs)} sources, all {self.nplanes} planes, {len(bands)} row "
+                          f"bands on {cores} threads; PatchMatch: {ncrop} 64x48 crops x 1 iteration from the true "
+                          f"depth; full step extrapolated per evaluation ({t_full:.1f} s)"}
+
+
+def cpu_baseline(cfg, nplanes, iters, device="cpu"):
+    return CpuSample(cfg, nplanes, iters, device=device).measure()
 
 
 # ------------------------------------------------------------------ reference arm
 def run_reference(a):
+    """The reference's own CPU implementation of the path (oracle/_ref), each step one timed pass
+    over the bounded sample (CpuSample); rank 0 only, the other ranks exit without work."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cfg, W, H, nplanes, iters = workload(a)
+    sample = CpuSample(cfg, nplanes, iters)
     for _ in range(a.warmup):
-        pass
-    vals = []
+        sample.measure()
+    vals, step_s = [], []
     last = None
     for _ in range(a.steps):
-        last = cpu_baseline(cfg, nplanes, iters, budget_s=10.0)
+        last = sample.measure()
         vals.append(last["value"])
+        step_s.append(last["step_s_extrapolated"])
     v = statistics.median(vals)
     line = {"metric": "ZNCC evaluations/s (pixel x plane x view), sweep + PatchMatch", "value": v,
             "unit": "Gpix.plane.view/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": statistics.median(step_s) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64 (reference CPU)",
             "data": "synthetic seeded heightfield scene",
-            "config": {"workload": cfg.name, "width": W, "height": H, "planes": nplanes, "pm_iters": iters},
+            "config": {"workload": cfg.name, "width": W, "height": H, "sources": len(sample.srcs),
+                       "planes": nplanes, "window": 2 * cfg.radius + 1, "top_k": cfg.top_k, "pm_iters": iters,
+                       "pm_window": 2 * cfg.pm_radius + 1},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "Gpix.plane.view/s", "cores": last["cores"], "kind": last["kind"],
-                             "sample": last["sample"]},
+                             "sample": last["sample"] + "; ms_per_step is the extrapolated full step"},
             "e2e": {"value": v, "unit": "Gpix.plane.view/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 

@@ -119,8 +119,9 @@ mvs_status mvs_sweep(const mvs_sweep_args* args, void* stream);
  * plane-chunk scratch is one 32 MiB file-scope device array per GPU, held until the process
  * exits: with plane_chunks = 0 the chunk count is lowered until the records fit; an explicit
  * plane_chunks whose records (6 floats per pixel per chunk) exceed 32 MiB gives MVS_ERR_VALUE.
- * The first call on a device looks the array up (with that device current): make it before
- * any stream capture. All calls share the array and it keeps the last call's contents (none of
+ * Every call looks the array's address up on the current device; the first call on a device
+ * (and the first after its context was reset) loads the array there: make it before any stream
+ * capture. All calls share the array and it keeps the last call's contents (none of
  * it needs to start at zero); calls that overlap on the GPU race on it. Calls no cudaMalloc,
  * cudaFree or other allocating routine. */
 mvs_status mvs_sweep_noalloc(const mvs_sweep_args* args, void* stream);
@@ -181,6 +182,39 @@ mvs_status mvs_depth_view(int32_t h, int32_t w, const uint8_t* rgb, const float*
 mvs_status mvs_half(int32_t planes, int32_t h, int32_t w, const float* in, float* out,
                     void* stream);
 
+/* Camera-axis depth of every tie point that lands inside a view: X (n, 3) world points (device),
+ * `cam` a HOST camera row R(9) C(3) f k1 k2 k3 cx cy, pinhole map u = f x / z + cx, v = f y / z + cy;
+ * out[i] = z_i where z_i > 0, 0 <= u < w and 0 <= v < h, else NaN (device, float64). The census
+ * of densify._depth_range (densify.py:208-230; the host takes its percentiles), float64 in the
+ * reference's NumPy / BLAS rounding order. */
+mvs_status mvs_tie_depths(int32_t n, const double* X, const double* cam, int32_t w, int32_t h, double* out,
+                          void* stream);
+
+#define MVS_BAND_MIN_POINTS 50    /* fewer observed tie points: the band is the view's whole range */
+
+typedef struct mvs_depth_band_args {
+    int32_t H, W;                          /* sweep image (the coarse pyramid level)            */
+    int32_t block;                         /* cell side in pixels                               */
+    int32_t n_pts;                         /* tie points the view observes                      */
+    const double* X;                       /* DEVICE (n_pts, 3) world points                    */
+    const double* cam;                     /* HOST 18: the view's camera row at this level      */
+    double lo, hi;                         /* the view's depth range (metres)                   */
+    double margin;                         /* metres added on each side of a cell's range       */
+    int32_t nd, pad_;                      /* hypotheses of the sweep over the band             */
+    float* base;                           /* out (H, W): 1 / hi_px, inverse depth of hyp. 0   */
+    float* step;                           /* out (H, W): (1 / max(lo_px, 1e-6) - base) / max(nd - 1, 1) */
+    float* inv_hi;                         /* out (H, W) 1 / max(lo_px, 1e-6), or NULL          */
+} mvs_depth_band_args;
+
+/* Per-pixel inverse-depth band of the coarse sweep from the tie points the view observes, and
+ * the linear hypothesis maps over it (densify._depth_band, densify.py:233-274, and the step map
+ * of densify.depth_map, :409-411): the points are scattered into block x block cells (count,
+ * min and max depth); a cell with >= 5 points takes the extent of its 3 x 3 neighbourhood's
+ * counted cells, widened by margin + 5 % and clipped to [lo, hi]; other cells (and every cell
+ * when n_pts < MVS_BAND_MIN_POINTS) take [lo, hi]. Bit-identical to the reference's NumPy
+ * values. Allocates its cell table stream-ordered. */
+mvs_status mvs_depth_band(const mvs_depth_band_args* args, void* stream);
+
 /* float32 -> FP16 image conversion for MVS_PREC_FP16 sources (round to nearest; NaN kept). */
 mvs_status mvs_to_fp16(int64_t n, const float* in, void* out_half, void* stream);
 
@@ -216,18 +250,33 @@ typedef struct mvs_pm_args {
     int32_t r, step, top_k, iters;
     double geo_w, geo_tol, dmin, dmax;
     uint32_t seed;
-    int32_t it0;                           /* first iteration index (resumable jobs), usually 0 */
+    int32_t it0;                           /* first iteration index (resumable jobs), usually 0;
+                                              sets the trial scales 0.05 / (it0 + it + 1) and
+                                              0.3 / (it0 + it + 1)                              */
     int64_t* changed;                      /* DEVICE int64 counter, incremented (may be NULL)   */
+    uint32_t* rng_state;                   /* DEVICE uint32 or NULL: the xorshift32 state of the
+                                              random trials' stream. NULL: the stream starts at
+                                              seed | 1, as the reference's pm_refine does per
+                                              call. Otherwise it starts at *rng_state and the
+                                              state after the call is written back, so a job
+                                              split over calls (it0) draws what one call would
+                                              (initialise it to seed | 1)                       */
 } mvs_pm_args;
 
 /* Red-black slanted-plane PatchMatch (_dense.pm_refine, _dense.pyx:566-666). Same cost,
- * propagation pattern, trial scales and acceptance rule; the random trials draw from a
- * counter-based generator keyed by (seed, iteration, pixel, draw) instead of one sequential
- * xorshift stream, so both colours of every iteration update in parallel. */
+ * propagation pattern, trial scales and acceptance rule, and the reference's own random stream:
+ * one xorshift32 sequence (_dense.pyx:559-563) from which every active pixel whose depth is
+ * finite after propagation takes 8 draws in raster order, colour pass after colour pass. Each
+ * pass runs propagation for all its pixels in parallel, counts the drawing pixels (a prefix sum
+ * in raster order) and jumps the stream to each pixel's offset (GF(2) matrix powers), then runs
+ * the trials in parallel. With MVS_PM_FP64 the result is bit-identical to the reference's.
+ * Scratch (about 21 bytes per pixel, plus 16 per pixel when iters > 1) is allocated
+ * stream-ordered per call. */
 mvs_status mvs_pm_refine(const mvs_pm_args* args, void* stream);
 
-/* The counter-based draw used by mvs_pm_refine: uniform in [0, 1) with 24-bit resolution. */
-double mvs_pm_uniform(uint32_t seed, int32_t it, int64_t pixel, int32_t draw);
+/* The xorshift32 state after n steps of the PatchMatch stream from `state` (host; jump-ahead by
+ * GF(2) matrix powers, n up to 2^64 - 1). mvs_pm_refine's trials use the same jumps. */
+uint32_t mvs_pm_stream_advance(uint32_t state, uint64_t n);
 
 /* ---------------------------------------------------------------- batched sweep */
 
@@ -397,6 +446,13 @@ mvs_status mvs_sgm(int32_t D, int32_t H, int32_t W, const float* cost, float P1,
  * state untouched and is counted here). Synchronises with the device; clears the count.
  * Returns MVS_ERR_TIMEOUT when the count was non-zero. No counterpart in the reference. */
 mvs_status mvs_device_faults(uint32_t* count);
+
+/* Iterations of the sweep's bounded wait for its reference-tile copy (default 2^20 try_wait
+ * iterations, far above a copy's latency); returns the previous value. For tests of the give-up
+ * path: with 0 every tile gives up at once - it counts a fault, waits (with the default bound)
+ * for its copy in flight to land and returns with its state untouched. Applies to calls made
+ * after it, from any thread. No counterpart in the reference. */
+uint32_t mvs_set_wait_limit(uint32_t iterations);
 
 /* Message of this thread's last failing call ("" if none). Returns the message length. */
 size_t mvs_last_error(char* buf, size_t cap);

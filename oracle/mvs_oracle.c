@@ -11,9 +11,8 @@
  *   oracle_ncc_warp         <- _dense.ncc_warp          (_dense.pyx:13-110)
  *   oracle_combine          <- _dense.combine           (_dense.pyx:113-144)
  *   oracle_box_zero_mean    <- _fast.box_zero_mean      (_fast.pyx:661-713)
- *   oracle_pm_refine        <- _dense.pm_refine         (_dense.pyx:405-666), with either the
- *                              reference's sequential xorshift32 draws (rng = 0) or the
- *                              counter-based draws of libmvs_b200's PatchMatch (rng = 1)
+ *   oracle_pm_refine        <- _dense.pm_refine         (_dense.pyx:405-666), with the
+ *                              reference's sequential xorshift32 draws (_rnd, :559-563)
  *   oracle_consistency      <- densify._consistency     (densify.py:441-478; _fast.pyx:201-268)
  *   oracle_init_normals     <- densify._init_normals    (densify.py:481-496)
  *   oracle_fuse_view        <- one reference image of densify._fuse_loop (densify.py:688-762;
@@ -531,39 +530,20 @@ static double rnd_xorshift(uint32_t* st)
     return (st[0] & 0xFFFFFF) / 16777216.0;
 }
 
-static uint64_t mix64(uint64_t x)
-{
-    x ^= x >> 30;
-    x *= 0xBF58476D1CE4E5B9ULL;
-    x ^= x >> 27;
-    x *= 0x94D049BB133111EBULL;
-    x ^= x >> 31;
-    return x;
-}
-
-/* the counter-based draw of libmvs_b200's PatchMatch, restated */
-EXPORT double oracle_pm_uniform(uint32_t seed, int it, int64_t pixel, int draw)
-{
-    uint64_t x = mix64((uint64_t)seed + 0x9E3779B97F4A7C15ULL);
-    x = mix64(x ^ ((uint64_t)(uint32_t)it * 0xD1B54A32D192ED03ULL));
-    x = mix64(x ^ ((uint64_t)pixel * 0x8CB92BA72F3D8DD7ULL));
-    x = mix64(x ^ (uint64_t)(uint32_t)draw);
-    return (double)(uint32_t)(x >> 40) / 16777216.0;
-}
-
-/* rng = 0: the reference's single xorshift32 stream (seed | 1); rng = 1: counter-based draws
- * keyed by (seed | 1, it0 + it, pixel, 4 trial + component). Returns the change count. */
+/* The stream carried across calls: state NULL starts at seed | 1 as the reference does; otherwise
+ * the stream starts at *state and the state after the call's draws is written back (a job split
+ * over calls with it0 = iterations done). Returns the change count. */
 EXPORT int64_t oracle_pm_refine(int H, int W, const float* ref, const float* ray, const double* Cr, int S,
                                 const float* const* srcs, const float* const* src_depths, const int* src_h,
                                 const int* src_w, const double* par, float* depth, float* normal, float* score,
                                 const unsigned char* active, int r, int step, int top_k, double geo_w, double geo_tol,
-                                int iters, double dmin, double dmax, uint32_t seed, int rng, int it0)
+                                int iters, double dmin, double dmax, uint32_t seed, uint32_t* state, int it0)
 {
     static const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
     static const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
     const ptrdiff_t HW = (ptrdiff_t)H * W;
     pm_ctx c;
-    uint32_t st = seed | 1u;
+    uint32_t st = state ? *state : (seed | 1u);
     int64_t changed = 0;
     int it, colour, y, x, k, tr;
     if (S == 0 || S > 16) return 0;
@@ -611,14 +591,7 @@ EXPORT int64_t oracle_pm_refine(int H, int W, const float* ref, const float* ray
                     if (isfinite(depth[idx])) {
                         for (tr = 0; tr < 2; tr++) {
                             double u0, u1, u2, u3, dp, nn;
-                            if (rng == 0) {
-                                u0 = rnd_xorshift(&st); u1 = rnd_xorshift(&st); u2 = rnd_xorshift(&st); u3 = rnd_xorshift(&st);
-                            } else {
-                                u0 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 0);
-                                u1 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 1);
-                                u2 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 2);
-                                u3 = oracle_pm_uniform(seed | 1u, git, idx, 4 * tr + 3);
-                            }
+                            u0 = rnd_xorshift(&st); u1 = rnd_xorshift(&st); u2 = rnd_xorshift(&st); u3 = rnd_xorshift(&st);
                             dp = depth[idx] * (1 + dd_scale * (2 * u0 - 1));
                             nb[0] = normal[idx] + nn_scale * (2 * u1 - 1);
                             nb[1] = normal[HW + idx] + nn_scale * (2 * u2 - 1);
@@ -641,6 +614,7 @@ EXPORT int64_t oracle_pm_refine(int H, int W, const float* ref, const float* ray
             }
         }
     }
+    if (state) *state = st;
     return changed;
 }
 

@@ -57,8 +57,7 @@ def lib() -> C.CDLL:
         L.oracle_pm_refine.restype = C.c_int64
         L.oracle_pm_refine.argtypes = [C.c_int, C.c_int, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp,
                                        vp, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_int,
-                                       C.c_double, C.c_double, C.c_uint32, C.c_int, C.c_int]
-        L.oracle_pm_uniform.restype = C.c_double
+                                       C.c_double, C.c_double, C.c_uint32, vp, C.c_int]
         L.oracle_consistency.restype = None
         L.oracle_consistency.argtypes = [C.c_int, C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp, C.c_double, vp, vp, vp,
                                          C.c_double, C.c_int, vp]
@@ -74,7 +73,6 @@ def lib() -> C.CDLL:
                                        C.c_int, C.c_int, vp, vp, vp]
         L.oracle_init_normals.restype = None
         L.oracle_init_normals.argtypes = [C.c_int, C.c_int, vp, vp, vp]
-        L.oracle_pm_uniform.argtypes = [C.c_uint32, C.c_int, C.c_int64, C.c_int]
         _lib = L
     return _lib
 
@@ -249,9 +247,10 @@ def sweep_fp64(ref, srcs, ray, geo, hyps, r, top_k):
 
 # ------------------------------------------------------------------ PatchMatch
 def pm_refine(ref, ray, Cr, srcs, src_depths, par, depth, normal, score, active, r, step, top_k, geo_w, geo_tol,
-              iters, dmin, dmax, seed, rng=1, it0=0) -> int:
-    """_dense.pm_refine (_dense.pyx:566-666) restated, in place. rng=0: the reference's xorshift
-    stream; rng=1: libmvs_b200's counter-based draws."""
+              iters, dmin, dmax, seed, it0=0, state=None) -> int:
+    """_dense.pm_refine (_dense.pyx:566-666) restated, in place, with the reference's xorshift32
+    stream. state: None (start at seed | 1, as the reference) or a 1-element uint32 array carried
+    from call to call (in: the stream state to start at; out: the state after the draws)."""
     H, W = ref.shape
     S = len(srcs)
     srcs = [_f32(s) for s in srcs]
@@ -264,15 +263,24 @@ def pm_refine(ref, ray, Cr, srcs, src_depths, par, depth, normal, score, active,
     Cr = _f64(Cr)
     for a, t in ((depth, np.float32), (normal, np.float32), (score, np.float32)):
         assert a.dtype == t and a.flags.c_contiguous
+    if state is not None:
+        assert state.dtype == np.uint32 and state.size == 1 and state.flags.c_contiguous
     act = np.ascontiguousarray(active, np.uint8)
     return int(lib().oracle_pm_refine(H, W, _p(_f32(ref)), _p(_f32(ray)), _p(Cr), S, sp, dpp, _p(hs), _p(ws),
                                       _p(par), _p(depth), _p(normal), _p(score), _p(act), int(r), int(step),
                                       int(top_k), float(geo_w), float(geo_tol), int(iters), float(dmin), float(dmax),
-                                      int(seed) & 0xFFFFFFFF, int(rng), int(it0)))
+                                      int(seed) & 0xFFFFFFFF, None if state is None else _p(state), int(it0)))
 
 
-def pm_uniform(seed: int, it: int, pixel: int, draw: int) -> float:
-    return float(lib().oracle_pm_uniform(seed & 0xFFFFFFFF, it, pixel, draw))
+def xorshift_steps(state: int, n: int) -> int:
+    """n sequential steps of the reference's xorshift32 (_dense.pyx:559-563): the checker of the
+    device stream's jump-ahead."""
+    s = int(state) & 0xFFFFFFFF
+    for _ in range(int(n)):
+        s ^= (s << 13) & 0xFFFFFFFF
+        s ^= s >> 17
+        s ^= (s << 5) & 0xFFFFFFFF
+    return s
 
 
 # ------------------------------------------------------------------ pass-2 geometry

@@ -20,6 +20,7 @@ LIB_PATH = os.path.join(HERE, "libmvs_b200.so")
 MAX_SOURCES = 16
 MAX_RADIUS = 7
 MAX_PLANES_PER_CALL = 1024
+BAND_MIN_POINTS = 50
 
 OK, ERR_VALUE, ERR_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(6)
 HYP_MAPS, HYP_LINEAR, HYP_REFINE, HYP_PLANES = range(4)
@@ -50,7 +51,7 @@ class PMArgs(C.Structure):
                 ("src_w", i32 * MAX_SOURCES), ("par", vp), ("depth", vp), ("normal", vp), ("score", vp),
                 ("active", vp), ("r", i32), ("step", i32), ("top_k", i32), ("iters", i32),
                 ("geo_w", C.c_double), ("geo_tol", C.c_double), ("dmin", C.c_double), ("dmax", C.c_double),
-                ("seed", C.c_uint32), ("it0", i32), ("changed", vp)]
+                ("seed", C.c_uint32), ("it0", i32), ("changed", vp), ("rng_state", vp)]
 
 
 class ConsArgs(C.Structure):
@@ -81,6 +82,12 @@ class HeightScoreArgs(C.Structure):
                 ("st", vp), ("ref", vp)]
 
 
+class DepthBandArgs(C.Structure):
+    _fields_ = [("H", i32), ("W", i32), ("block", i32), ("n_pts", i32), ("X", vp), ("cam", vp), ("lo", C.c_double),
+                ("hi", C.c_double), ("margin", C.c_double), ("nd", i32), ("pad_", i32), ("base", vp), ("step", vp),
+                ("inv_hi", vp)]
+
+
 class BatchJob(C.Structure):
     _fields_ = [("sweep", SweepArgs), ("depth", vp)]
 
@@ -104,8 +111,10 @@ SIGNATURES = {
     "mvs_depth_view": (i32, [i32, i32, vp, vp, vp, vp, vp, vp, vp]),
     "mvs_half": (i32, [i32, i32, i32, vp, vp, vp]),
     "mvs_to_fp16": (i32, [i64, vp, vp, vp]),
+    "mvs_tie_depths": (i32, [i32, vp, vp, i32, i32, vp, vp]),
+    "mvs_depth_band": (i32, [vp, vp]),
     "mvs_pm_refine": (i32, [vp, vp]),
-    "mvs_pm_uniform": (C.c_double, [C.c_uint32, i32, i64, i32]),
+    "mvs_pm_stream_advance": (C.c_uint32, [C.c_uint32, C.c_uint64]),
     "mvs_batch_create": (i32, [vp, i32, vp, vp]),
     "mvs_batch_run": (i32, [vp, i32, vp]),
     "mvs_batch_stats": (i32, [vp, vp, vp]),
@@ -123,6 +132,7 @@ SIGNATURES = {
     "mvs_sgm": (i32, [i32, i32, i32, vp, C.c_float, C.c_float, vp, vp]),
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_device_faults": (i32, [vp]),
+    "mvs_set_wait_limit": (C.c_uint32, [C.c_uint32]),
     "mvs_version": (C.c_char_p, []),
 }
 
@@ -170,6 +180,14 @@ def check(status: int, what: str = "") -> None:
     if status == ERR_UNSUPPORTED:
         raise NotImplementedError(msg)
     raise RuntimeError(msg)
+
+
+def check_device_faults() -> None:
+    """Raises TimeoutError when a bounded device-side wait gave up since the last check (the
+    sweep's wait for its reference-tile copy: such tiles keep their previous state). Synchronises
+    with the device; clears the count."""
+    n = C.c_uint32(0)
+    check(load().mvs_device_faults(C.byref(n)), "device faults")
 
 
 def stream_handle(stream=None) -> int:

@@ -198,6 +198,124 @@ __global__ void to_fp16_kernel(long long n, const float* __restrict__ in, __half
     out[o] = __float2half_rn(in[o]);
 }
 
+// ---- tie-point geometry of the coarse-to-fine driver (densify._depth_range / _depth_band)
+
+// Camera coordinates of a world point as NumPy's (X - C) @ R^T: OpenBLAS's dgemm accumulates each
+// output as a = d0 r0; a = fma(d1, r1, a); a = fma(d2, r2, a).
+__device__ __forceinline__ void tie_cam_coords(const double* cam, const double* X, double* xc) {
+    const double d0 = __dsub_rn(X[0], cam[9]), d1 = __dsub_rn(X[1], cam[10]), d2 = __dsub_rn(X[2], cam[11]);
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        xc[j] = __fma_rn(d2, cam[3 * j + 2], __fma_rn(d1, cam[3 * j + 1], __dmul_rn(d0, cam[3 * j])));
+}
+
+struct TieCam {
+    double c[18];   // R(9) C(3) f k1 k2 k3 cx cy
+};
+
+// One tie point: its camera-axis depth if it lands inside the w x h view under the pinhole map
+// u = f x / z + cx (the range census), else NaN.
+__global__ void tie_depths_kernel(int n, const double* __restrict__ X, const TieCam cam, int w, int h,
+                                  double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double xc[3];
+    tie_cam_coords(cam.c, X + 3LL * i, xc);
+    const double f = cam.c[12], cx = cam.c[16], cy = cam.c[17];
+    const double u = __dadd_rn(__ddiv_rn(__dmul_rn(f, xc[0]), xc[2]), cx);
+    const double v = __dadd_rn(__ddiv_rn(__dmul_rn(f, xc[1]), xc[2]), cy);
+    const bool in = xc[2] > 0.0 && u >= 0.0 && v >= 0.0 && u < (double)w && v < (double)h;
+    out[i] = in ? xc[2] : __longlong_as_double(0x7ff8000000000000LL);
+}
+
+// NumPy's floor division of a non-negative double by a positive integer: exact (the remainder
+// from fmod is exact, so a - fmod(a, b) is a multiple of b).
+__device__ __forceinline__ int floor_div_pos(double a, int b) {
+    const double bd = (double)b;
+    return (int)__ddiv_rn(__dsub_rn(a, fmod(a, bd)), bd);
+}
+
+// Scatter of the observed tie points into block x block cells of the sweep image: per cell the
+// count and the min / max camera depth. Depths are > 0 here, so their bit patterns order like the
+// values and the extrema are integer atomics (order-independent: the same cell values in any
+// order).
+__global__ void band_scatter_kernel(int n, const double* __restrict__ X, const TieCam cam, int H, int W, int block,
+                                    int gw, unsigned long long* __restrict__ zlo, unsigned long long* __restrict__ zhi,
+                                    int* __restrict__ cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double xc[3];
+    tie_cam_coords(cam.c, X + 3LL * i, xc);
+    if (!(xc[2] > 0.0)) return;
+    // _Cam.project_cam: pinhole + radial k1..k3, z floored at 1e-6
+    const double* c = cam.c;
+    const double z = fmax(xc[2], 1e-6);
+    const double x = __ddiv_rn(xc[0], z), y = __ddiv_rn(xc[1], z);
+    const double r2 = __dadd_rn(__dmul_rn(x, x), __dmul_rn(y, y));
+    const double poly =
+        __dadd_rn(1.0, __dmul_rn(r2, __dadd_rn(c[13], __dmul_rn(r2, __dadd_rn(c[14], __dmul_rn(r2, c[15]))))));
+    const double d = __dmul_rn(c[12], poly);
+    const double u = __dadd_rn(__dmul_rn(d, x), c[16]), v = __dadd_rn(__dmul_rn(d, y), c[17]);
+    if (!(u >= 0.0 && v >= 0.0 && u < (double)W && v < (double)H)) return;
+    const int bx = floor_div_pos(fmin(u, (double)(W - 1)), block);
+    const int by = floor_div_pos(fmin(v, (double)(H - 1)), block);
+    const int b = by * gw + bx;
+    const unsigned long long zb = (unsigned long long)__double_as_longlong(xc[2]);
+    atomicMin(zlo + b, zb);
+    atomicMax(zhi + b, zb);
+    atomicAdd(cnt + b, 1);
+}
+
+__global__ void band_init_kernel(int nb, unsigned long long* zlo, unsigned long long* zhi, int* cnt) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    zlo[i] = 0x7FF0000000000000ULL;   // +inf
+    zhi[i] = 0ULL;                    // +0 (every scattered depth is larger)
+    cnt[i] = 0;
+}
+
+// Per pixel: the band of its cell. A cell with >= 5 points takes the depth extent of the points
+// in its 3 x 3 cell neighbourhood (cells with >= 5 points only), widened by margin + 5 % of that
+// extent and clipped to the view's range; other cells take the view's range. Out: float32
+// base = 1 / hi and step = (1 / max(lo, 1e-6) - base) / max(nd - 1, 1) of the coarse sweep.
+__global__ void band_fill_kernel(int H, int W, int block, int gh, int gw, const unsigned long long* __restrict__ zlo,
+                                 const unsigned long long* __restrict__ zhi, const int* __restrict__ cnt, double lo_g,
+                                 double hi_g, double margin, int nd, int uniform, float* __restrict__ base,
+                                 float* __restrict__ step, float* __restrict__ inv_hi) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= W || y >= H) return;
+    float il, ih;
+    if (uniform) {
+        il = __double2float_rn(__ddiv_rn(1.0, hi_g));
+        ih = __double2float_rn(__ddiv_rn(1.0, lo_g));
+    } else {
+        const int bx = x / block, by = y / block;
+        double lo3 = __longlong_as_double(0x7FF0000000000000LL), hi3 = -lo3;
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int cy = by + dy, cx = bx + dx;
+                if (cy < 0 || cx < 0 || cy >= gh || cx >= gw) continue;
+                const int b = cy * gw + cx;
+                if (cnt[b] < 5) continue;
+                lo3 = fmin(lo3, __longlong_as_double((long long)zlo[b]));
+                hi3 = fmax(hi3, __longlong_as_double((long long)zhi[b]));
+            }
+        const bool has = cnt[by * gw + bx] >= 5 && isfinite(lo3) && isfinite(hi3);
+        double lob = lo_g, hib = hi_g;
+        if (has) {
+            const double pad = __dadd_rn(margin, __dmul_rn(0.05, __dsub_rn(hi3, lo3)));
+            lob = fmin(fmax(__dsub_rn(lo3, pad), lo_g), hi_g);
+            hib = fmin(fmax(__dadd_rn(hi3, pad), lo_g), hi_g);
+        }
+        il = __double2float_rn(__ddiv_rn(1.0, hib));
+        ih = __double2float_rn(__ddiv_rn(1.0, fmax(lob, 1e-6)));
+    }
+    const long long o = (long long)y * W + x;
+    base[o] = il;
+    step[o] = __fdiv_rn(__fsub_rn(ih, il), (float)max(nd - 1, 1));
+    if (inv_hi) inv_hi[o] = ih;
+}
+
 static inline unsigned blocks(long long n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace mvs
@@ -305,4 +423,51 @@ extern "C" mvs_status mvs_to_fp16(int64_t n, const float* in, void* out, void* s
     if (!in || !out) return fail(MVS_ERR_VALUE, "to_fp16: null pointer");
     to_fp16_kernel<<<blocks(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(n, in, reinterpret_cast<__half*>(out));
     return check_launch("to_fp16");
+}
+
+extern "C" mvs_status mvs_tie_depths(int32_t n, const double* X, const double* cam, int32_t w, int32_t h, double* out,
+                                     void* stream) {
+    clear_error();
+    if (n < 0 || w < 0 || h < 0) return fail(MVS_ERR_VALUE, "tie_depths: negative size");
+    if (n == 0) return MVS_OK;
+    if (!X || !cam || !out) return fail(MVS_ERR_VALUE, "tie_depths: null pointer");
+    TieCam c;
+    memcpy(c.c, cam, sizeof(c.c));
+    tie_depths_kernel<<<blocks(n, 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(n, X, c, w, h, out);
+    return check_launch("tie_depths");
+}
+
+extern "C" mvs_status mvs_depth_band(const mvs_depth_band_args* a, void* stream) {
+    clear_error();
+    if (!a) return fail(MVS_ERR_VALUE, "depth_band: null arguments");
+    if (a->H < 0 || a->W < 0 || a->n_pts < 0) return fail(MVS_ERR_VALUE, "depth_band: negative size");
+    if (a->block < 1) return fail(MVS_ERR_VALUE, "depth_band: block must be >= 1");
+    if (a->H == 0 || a->W == 0) return MVS_OK;
+    if (!a->cam || !a->base || !a->step || (a->n_pts >= MVS_BAND_MIN_POINTS && !a->X))
+        return fail(MVS_ERR_VALUE, "depth_band: null pointer");
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int gh = (a->H + a->block - 1) / a->block, gw = (a->W + a->block - 1) / a->block;
+    const int nb = gh * gw;
+    const bool uniform = a->n_pts < MVS_BAND_MIN_POINTS;
+    char* cells = nullptr;
+    if (!uniform) {
+        MVS_CUDA(cudaMallocAsync((void**)&cells, (size_t)nb * 20, st), "depth_band: cell table");
+        unsigned long long* zlo = reinterpret_cast<unsigned long long*>(cells);
+        unsigned long long* zhi = zlo + nb;
+        int* cnt = reinterpret_cast<int*>(zhi + nb);
+        TieCam c;
+        memcpy(c.c, a->cam, sizeof(c.c));
+        band_init_kernel<<<blocks(nb, 256), 256, 0, st>>>(nb, zlo, zhi, cnt);
+        band_scatter_kernel<<<blocks(a->n_pts, 256), 256, 0, st>>>(a->n_pts, a->X, c, a->H, a->W, a->block, gw, zlo,
+                                                                   zhi, cnt);
+    }
+    const unsigned long long* zlo = reinterpret_cast<const unsigned long long*>(cells);
+    const unsigned long long* zhi = uniform ? nullptr : zlo + nb;
+    const int* cnt = uniform ? nullptr : reinterpret_cast<const int*>(zhi + nb);
+    band_fill_kernel<<<dim3(blocks(a->W, 256), a->H), 256, 0, st>>>(a->H, a->W, a->block, gh, gw, zlo, zhi, cnt, a->lo,
+                                                                   a->hi, a->margin, a->nd, uniform ? 1 : 0, a->base,
+                                                                   a->step, a->inv_hi);
+    const mvs_status s = check_launch("depth_band");
+    if (cells) cudaFreeAsync(cells, st);
+    return s;
 }

@@ -12,13 +12,14 @@
 //     life of the process;
 //   * with plane_chunks == 0 the chunk count is the automatic one, lowered until the records fit;
 //     an explicit plane_chunks whose records do not fit is rejected (MVS_ERR_VALUE);
-//   * the first call on a device looks up the array's device address (cudaGetSymbolAddress,
-//     with that device current); make that first call before any stream capture;
+//   * every call looks up the array's device address on the current device
+//     (cudaGetSymbolAddress, which allocates nothing once the array exists); the first call on a
+//     device - and the first after that device's context was reset - loads the library's device
+//     code there, which is when the array is created: make that first call before any stream
+//     capture;
 //   * every call shares the array and it keeps the last call's contents; nothing in it needs to
 //     start at zero (each chunk record is written in full before it is merged), but calls that
 //     overlap on the GPU (different streams, or host threads without ordering) race on it.
-#include <mutex>
-
 #include "sweep_tile.cuh"
 
 #define MVS_NOALLOC_SCRATCH_BYTES (32u << 20)
@@ -30,24 +31,15 @@ mvs_status sweep_with_scratch(const mvs_sweep_args* a, void* scratch, size_t scr
 
 static __device__ __align__(256) float g_noalloc_scratch[MVS_NOALLOC_SCRATCH_BYTES / sizeof(float)];
 
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_addr[128];        // device address of the array, per device ordinal
-
-// The array's name is a host-side stand-in in host code; its device address must be looked up
-// per device, with that device current.
+// The array's name is a host-side stand-in in host code; its device address is looked up on the
+// current device at every call, so a context that was reset and recreated is never served a
+// stale address.
 static mvs_status noalloc_scratch(void** out) {
-    int dev = 0;
-    MVS_CUDA(cudaGetDevice(&dev), "sweep_noalloc: current device");
-    if (dev < 0 || dev >= 128) return fail(MVS_ERR_UNSUPPORTED, "sweep_noalloc: device ordinal %d above 127", dev);
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-        void* p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p)
-            return fail(MVS_ERR_CUDA, "sweep_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
-        g_noalloc_addr[dev] = p;
-    }
-    *out = g_noalloc_addr[dev];
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+        return fail(MVS_ERR_CUDA, "sweep_noalloc: cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    *out = p;
     return MVS_OK;
 }
 

@@ -2,15 +2,28 @@
 //
 // This file is compiled with -fmad=false: every float64 expression below is evaluated with one
 // rounding per operation in the written order, which is how the reference's C (x86-64, no FMA)
-// evaluates it. With the same random draws, results are bit-identical to a sequential CPU
-// evaluation of the same algorithm.
+// evaluates it. The float64 mode is bit-identical to the reference's pm_refine.
 //
 // Parallel schedule. The reference visits the pixels of one colour ((x + y) % 2) in raster order,
 // but every pixel reads only its own plane, pixels of the other colour (all 8 neighbour offsets,
 // (+-1, 0), (0, +-1), (+-5, 0), (0, +-5), have odd parity) and static inputs. So all pixels of a
-// colour are independent: one thread per pixel per colour pass, two passes per iteration.
-// The only sequential dependence in the reference is its xorshift32 stream (_dense.pyx:559-563);
-// here each draw comes from a counter-based hash of (seed, iteration, pixel, draw index).
+// colour are independent: one thread (or lane group) per pixel per colour pass.
+//
+// Random trials. The reference draws from ONE xorshift32 stream (_rnd, _dense.pyx:559-563,
+// started at seed | 1 per call, :606): 8 draws, in raster order, for every active pixel of the
+// colour whose depth is finite once propagation is done (:646-652). Which pixels draw is known
+// only after propagation, so a colour pass runs as
+//   1. propagation (pm_kernel / pm_lane_kernel, PHASE 0): current plane + 8 neighbour planes;
+//      the pixel's best cost, score and a flag "draws" go to per-pass scratch;
+//   2. the exclusive prefix count of drawing pixels in raster order (pm_count_kernel,
+//      pm_scan_kernel, pm_state_kernel): pixel p's first draw is stream element
+//      base + 8 * prefix(p); xorshift32 is linear over GF(2), so its state there is
+//      A^(8 prefix(p)) s_base with A the 32 x 32 step matrix, applied as a product of the
+//      precomputed powers A^(8 * 2^j) (jump-ahead for F2-linear generators: Haramoto,
+//      Matsumoto, Nishimura, Panneton, L'Ecuyer 2008); the pass advances the stream by 8 * total;
+//   3. the two random trials (PHASE 1) from the pixel's own stream state.
+// The stream state lives on the device from pass to pass (and, with mvs_pm_args.rng_state, from
+// call to call), so no step waits for the host.
 #include "common.cuh"
 
 namespace mvs {
@@ -18,7 +31,6 @@ namespace mvs {
 struct PMParams {
     int H, W, S, r, step, top_k, it, colour;
     double cr0, cr1, cr2, geo_w, geo_tol, dmin, dmax, dd_scale, nn_scale;
-    unsigned seed;
     const float* ref;
     const float* ray;
     float* depth;
@@ -28,6 +40,11 @@ struct PMParams {
     unsigned long long* changed;
     double* cost_cache;                // per pixel; NaN = recompute (valid within one call)
     double* score_cache;
+    // per colour pass, indexed by the pass's pixel number t = y * ceil(W / 2) + x / 2
+    unsigned char* flags;              // bit 0: the pixel draws; bits 1-4: propagation changes
+    double* pbest;                     // cost of the plane kept by propagation
+    double* psc;                       // its photo score
+    const unsigned* pstate;            // xorshift32 state before the pixel's first draw
     const float* img[MVS_MAX_SOURCES];
     const float* dep[MVS_MAX_SOURCES];
     int iw[MVS_MAX_SOURCES], ih[MVS_MAX_SOURCES];
@@ -36,22 +53,41 @@ struct PMParams {
     double bsrc[MVS_MAX_SOURCES * 3];   // R_s (C_ref - C_s)
 };
 
-__host__ __device__ inline unsigned long long mix64(unsigned long long x) {
-    x ^= x >> 30;
-    x *= 0xBF58476D1CE4E5B9ULL;
-    x ^= x >> 27;
-    x *= 0x94D049BB133111EBULL;
-    x ^= x >> 31;
-    return x;
+// ---------------------------------------------------------------- the reference's stream
+
+// _rnd (_dense.pyx:559-563): one xorshift32 step, then the low 24 bits as a uniform in [0, 1).
+__host__ __device__ __forceinline__ unsigned xs_step(unsigned s) {
+    s ^= s << 13;
+    s ^= s >> 17;
+    s ^= s << 5;
+    return s;
+}
+__device__ __forceinline__ double xs_draw(unsigned& s) {
+    s = xs_step(s);
+    return (double)(s & 0xFFFFFFu) / 16777216.0;
 }
 
-// Uniform draw in [0, 1) with 24-bit resolution (the reference's _rnd resolution).
-__host__ __device__ inline double pm_uniform(unsigned seed, int it, long long pixel, int draw) {
-    unsigned long long x = mix64((unsigned long long)seed + 0x9E3779B97F4A7C15ULL);
-    x = mix64(x ^ ((unsigned long long)(unsigned)it * 0xD1B54A32D192ED03ULL));
-    x = mix64(x ^ ((unsigned long long)pixel * 0x8CB92BA72F3D8DD7ULL));
-    x = mix64(x ^ (unsigned long long)(unsigned)draw);
-    return (double)(unsigned)(x >> 40) / 16777216.0;
+// A 32 x 32 matrix over GF(2) by columns: col[i] = M e_i, so M s = XOR of col[i] over set bits i.
+struct Gf2 {
+    unsigned col[32];
+};
+__host__ __device__ __forceinline__ unsigned gf2_apply(const Gf2& m, unsigned s) {
+    unsigned r = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) r ^= m.col[i] & (0u - ((s >> i) & 1u));
+    return r;
+}
+
+// Jump table of the stream: t[j] = A^(8 * 2^j), A = one xorshift32 step.
+struct PMJump {
+    Gf2 t[32];
+};
+
+// State after 8 k steps from s.
+__device__ __forceinline__ unsigned jump8(const PMJump& J, unsigned s, unsigned k) {
+    for (int j = 0; k != 0; ++j, k >>= 1)
+        if (k & 1u) s = gf2_apply(J.t[j], s);
+    return s;
 }
 
 // _proj (_dense.pyx:429-445): world point -> pixel and camera depth.
@@ -241,23 +277,95 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
 #ifndef PM_MIN_BLOCKS
 #define PM_MIN_BLOCKS 8
 #endif
+// Pixel of pass number t (raster order of the colour's pixels): false past the image.
+__device__ __forceinline__ bool pm_pixel(const PMParams& c, long long t, int& y, int& x) {
+    const int half_w = (c.W + 1) / 2;
+    if (t >= (long long)c.H * half_w) return false;
+    y = (int)(t / half_w);
+    x = 2 * (int)(t - (long long)y * half_w) + ((y + c.colour) & 1);
+    return x < c.W;
+}
+
+// The two random trials of _dense.pyx:646-663 in the order of the reference: 4 draws per trial
+// (depth, then the three normal components), all 8 drawn even when a trial is skipped.
+template <typename CostFn>
+__device__ __forceinline__ void pm_trials(const PMParams& c, unsigned st, float& dcur, float* ncur, double& best,
+                                          double& sc, unsigned long long& changed, CostFn&& cost) {
+    for (int tr = 0; tr < 2; ++tr) {
+        const double u0 = xs_draw(st);
+        const double u1 = xs_draw(st);
+        const double u2 = xs_draw(st);
+        const double u3 = xs_draw(st);
+        const double dp = (double)dcur * (1.0 + c.dd_scale * (2.0 * u0 - 1.0));
+        double nb[3];
+        nb[0] = (double)ncur[0] + c.nn_scale * (2.0 * u1 - 1.0);
+        nb[1] = (double)ncur[1] + c.nn_scale * (2.0 * u2 - 1.0);
+        nb[2] = (double)ncur[2] + c.nn_scale * (2.0 * u3 - 1.0);
+        const double nn = sqrt(nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]);
+        if (nn < 1e-9 || dp < c.dmin || dp > c.dmax) continue;
+        nb[0] = nb[0] / nn;
+        nb[1] = nb[1] / nn;
+        nb[2] = nb[2] / nn;
+        double ph;
+        const double cst = cost(dp, nb, ph);
+        if (cst < best) {
+            best = cst;
+            sc = ph;
+            dcur = (float)dp;
+            ncur[0] = (float)nb[0];
+            ncur[1] = (float)nb[1];
+            ncur[2] = (float)nb[2];
+            ++changed;
+        }
+    }
+}
+
+// End of a pixel's visit: score, cost cache, change count (depth / normal written by the caller).
+__device__ __forceinline__ void pm_finish(const PMParams& c, long long idx, float dcur, double best, double sc,
+                                          unsigned long long changed) {
+    if (c.cost_cache) {
+        const bool keep = changed == 0 && isfinite(dcur);
+        c.cost_cache[idx] = keep ? best : __longlong_as_double(0x7ff8000000000000LL);
+        if (keep) c.score_cache[idx] = sc;
+    }
+    c.score[idx] = (float)sc;
+    if (changed && c.changed) atomicAdd(c.changed, changed);
+}
+
+// PHASE 0: current plane and propagation; PHASE 1: the random trials.
+template <int PHASE>
 __global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_constant__ PMParams c) {
-    const int H = c.H, W = c.W;
-    const int half_w = (W + 1) / 2;
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = (int)(t / half_w);
-    if (y >= H) return;
-    const int x = 2 * (int)(t - (long long)y * half_w) + ((y + c.colour) & 1);
-    if (x >= W) return;
-    const long long HW = (long long)H * W, idx = (long long)y * W + x;
-    if (!c.active[idx]) return;
-    const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
-    const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
+    int y, x;
+    const bool in = pm_pixel(c, t, y, x);
+    const long long HW = (long long)c.H * c.W, idx = (long long)y * c.W + x;
+    if (!in || !c.active[idx]) {
+        if (PHASE == 0 && t < (long long)c.H * ((c.W + 1) / 2)) c.flags[t] = 0;
+        return;
+    }
+    auto cost = [&](double d, const double* nb, double& ph) { return pm_cost(c, y, x, d, nb, ph); };
     float dcur = c.depth[idx];
     float ncur[3] = {c.normal[idx], c.normal[HW + idx], c.normal[2 * HW + idx]};
-    double n[3] = {ncur[0], ncur[1], ncur[2]};
     double best, sc, ncc;
     unsigned long long changed = 0;
+    if (PHASE == 1) {
+        const unsigned f = c.flags[t];
+        best = c.pbest[t];
+        sc = c.psc[t];
+        changed = f >> 1;
+        if (f & 1u) {
+            pm_trials(c, c.pstate[t], dcur, ncur, best, sc, changed, cost);
+            c.depth[idx] = dcur;
+            c.normal[idx] = ncur[0];
+            c.normal[HW + idx] = ncur[1];
+            c.normal[2 * HW + idx] = ncur[2];
+        }
+        pm_finish(c, idx, dcur, best, sc, changed);
+        return;
+    }
+    const int H = c.H, W = c.W;
+    const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
+    const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
     // cost of the pixel's current plane: reused from its previous visit when that visit kept the
     // plane it started with (the cost was then computed from these very float32 values)
     const double cached = c.cost_cache ? c.cost_cache[idx] : __longlong_as_double(0x7ff8000000000000LL);
@@ -265,6 +373,7 @@ __global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_con
         best = cached;
         sc = c.score_cache[idx];
     } else if (isfinite(dcur)) {
+        const double n[3] = {ncur[0], ncur[1], ncur[2]};
         best = pm_cost(c, y, x, (double)dcur, n, ncc);
         sc = ncc;
     } else {
@@ -295,45 +404,95 @@ __global__ void __launch_bounds__(128, PM_MIN_BLOCKS) pm_kernel(const __grid_con
             ++changed;
         }
     }
-    if (isfinite(dcur)) {
-        for (int tr = 0; tr < 2; ++tr) {
-            const double u0 = pm_uniform(c.seed, c.it, idx, 4 * tr + 0);
-            const double u1 = pm_uniform(c.seed, c.it, idx, 4 * tr + 1);
-            const double u2 = pm_uniform(c.seed, c.it, idx, 4 * tr + 2);
-            const double u3 = pm_uniform(c.seed, c.it, idx, 4 * tr + 3);
-            const double dp = (double)dcur * (1.0 + c.dd_scale * (2.0 * u0 - 1.0));
-            double nb[3];
-            nb[0] = (double)ncur[0] + c.nn_scale * (2.0 * u1 - 1.0);
-            nb[1] = (double)ncur[1] + c.nn_scale * (2.0 * u2 - 1.0);
-            nb[2] = (double)ncur[2] + c.nn_scale * (2.0 * u3 - 1.0);
-            const double nn = sqrt(nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]);
-            if (nn < 1e-9 || dp < c.dmin || dp > c.dmax) continue;
-            nb[0] = nb[0] / nn;
-            nb[1] = nb[1] / nn;
-            nb[2] = nb[2] / nn;
-            const double cst = pm_cost(c, y, x, dp, nb, ncc);
-            if (cst < best) {
-                best = cst;
-                sc = ncc;
-                dcur = (float)dp;
-                ncur[0] = (float)nb[0];
-                ncur[1] = (float)nb[1];
-                ncur[2] = (float)nb[2];
-                ++changed;
-            }
+    if (changed) {
+        c.depth[idx] = dcur;
+        c.normal[idx] = ncur[0];
+        c.normal[HW + idx] = ncur[1];
+        c.normal[2 * HW + idx] = ncur[2];
+    }
+    c.pbest[t] = best;
+    c.psc[t] = sc;
+    c.flags[t] = (unsigned char)((isfinite(dcur) ? 1u : 0u) | ((unsigned)changed << 1));
+}
+
+// ---------------------------------------------------------------- draw offsets of a colour pass
+
+constexpr int PM_SCAN_BLOCK = 1024;
+
+// Exclusive prefix sum over a block of PM_SCAN_BLOCK (32 warps) threads; `total` = the block's
+// sum. Called once per kernel (its shared words are not reused).
+__device__ __forceinline__ unsigned block_exclusive_scan(unsigned v, unsigned& total) {
+    __shared__ unsigned warp_off[32];
+    __shared__ unsigned tot_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    unsigned inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned u = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += u;
+    }
+    if (lane == 31) warp_off[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+        const unsigned wt = warp_off[lane];
+        unsigned wi = wt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned u = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += u;
         }
+        warp_off[lane] = wi - wt;
+        if (lane == 31) tot_s = wi;
     }
-    if (c.cost_cache) {
-        const bool keep = changed == 0 && isfinite(dcur);
-        c.cost_cache[idx] = keep ? best : __longlong_as_double(0x7ff8000000000000LL);
-        if (keep) c.score_cache[idx] = sc;
+    __syncthreads();
+    total = tot_s;
+    return warp_off[w] + inc - v;
+}
+
+// Drawing pixels per block of PM_SCAN_BLOCK pass pixels.
+__global__ void __launch_bounds__(PM_SCAN_BLOCK) pm_count_kernel(const unsigned char* flags, long long n,
+                                                                  unsigned* bsum) {
+    const long long t = (long long)blockIdx.x * PM_SCAN_BLOCK + threadIdx.x;
+    const int f = t < n ? (flags[t] & 1) : 0;
+    const int cnt = __syncthreads_count(f);
+    if (threadIdx.x == 0) bsum[blockIdx.x] = (unsigned)cnt;
+}
+
+// One block: block counts -> exclusive block offsets (in place); the stream state after the
+// pass's 8 * total draws goes to rng[nxt].
+__global__ void __launch_bounds__(PM_SCAN_BLOCK) pm_scan_kernel(unsigned* bsum, int nb, unsigned* rng, int cur,
+                                                                 int nxt, const __grid_constant__ PMJump J) {
+    const int per = (nb + PM_SCAN_BLOCK - 1) / PM_SCAN_BLOCK;
+    const int beg = min(nb, (int)threadIdx.x * per), end = min(nb, beg + per);
+    unsigned s = 0;
+    for (int i = beg; i < end; ++i) s += bsum[i];
+    unsigned total = 0;
+    unsigned run = block_exclusive_scan(s, total);
+    for (int i = beg; i < end; ++i) {
+        const unsigned v = bsum[i];
+        bsum[i] = run;
+        run += v;
     }
-    c.depth[idx] = dcur;
-    c.normal[idx] = ncur[0];
-    c.normal[HW + idx] = ncur[1];
-    c.normal[2 * HW + idx] = ncur[2];
-    c.score[idx] = (float)sc;
-    if (changed && c.changed) atomicAdd(c.changed, changed);
+    if (threadIdx.x == 0) rng[nxt] = jump8(J, rng[cur], total);
+}
+
+// Per drawing pixel: the stream state before its first draw (0 for pixels that do not draw; a
+// xorshift32 state is never 0).
+__global__ void __launch_bounds__(PM_SCAN_BLOCK) pm_state_kernel(const unsigned char* flags, long long n,
+                                                                  const unsigned* boff, const unsigned* rng, int cur,
+                                                                  const __grid_constant__ PMJump J, unsigned* pstate) {
+    const long long t = (long long)blockIdx.x * PM_SCAN_BLOCK + threadIdx.x;
+    const unsigned f = t < n ? (flags[t] & 1u) : 0u;
+    unsigned total;
+    const unsigned excl = block_exclusive_scan(f, total);
+    __shared__ unsigned base;
+    if (threadIdx.x == 0) base = jump8(J, rng[cur], boff[blockIdx.x]);
+    __syncthreads();
+    if (t < n) pstate[t] = f ? jump8(J, base, excl) : 0u;
+}
+
+__global__ void pm_rng_init_kernel(unsigned* rng, const unsigned* from, unsigned seed) {
+    rng[0] = from ? *from : seed;
 }
 
 // ---------------------------------------------------------------- float32 evaluation (MVS_PM_FP32)
@@ -669,20 +828,29 @@ __device__ __forceinline__ double pm_geo_lane(const PMParams& c, double d, doubl
 // Samples along one side of the window: offsets -r, -r + step, ... <= r.
 __host__ __device__ inline int pm_side(int r, int step) { return (2 * r) / step + 1; }
 
-template <int L, int NSIDE>
+// PHASE 0: current plane and propagation; PHASE 1: the random trials.
+template <int L, int NSIDE, int PHASE>
 __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const __grid_constant__ PMParams c) {
     extern __shared__ float4 pm_win[];
     const int H = c.H, W = c.W;
-    const int half_w = (W + 1) / 2;
     const int lane = threadIdx.x & (L - 1);
     const unsigned gmask = (L == 32 ? 0xffffffffu : ((1u << L) - 1u)) << (threadIdx.x & 31 & ~(L - 1));
     const long long t = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / L;
-    const int y = (int)(t / half_w);
-    if (y >= H) return;
-    const int x = 2 * (int)(t - (long long)y * half_w) + ((y + c.colour) & 1);
-    if (x >= W) return;
+    int y, x;
+    const bool in_img = pm_pixel(c, t, y, x);
     const long long HW = (long long)H * W, idx = (long long)y * W + x;
-    if (!c.active[idx]) return;
+    if (!in_img || !c.active[idx]) {
+        if (PHASE == 0 && lane == 0 && t < (long long)H * ((W + 1) / 2)) c.flags[t] = 0;
+        return;
+    }
+    unsigned pflag = 0;
+    if (PHASE == 1) {
+        pflag = c.flags[t];
+        if (!(pflag & 1u)) {           // no draws: the visit ends with propagation's result
+            if (lane == 0) pm_finish(c, idx, c.depth[idx], c.pbest[t], c.psc[t], pflag >> 1);
+            return;
+        }
+    }
     int ng = 0;
     for (int s = 0; s < c.S; ++s) ng += c.dep[s] != nullptr;
     const bool use_geo = c.geo_w > 0.0 && ng > 0;
@@ -763,12 +931,25 @@ __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const 
         const double geo = use_geo ? pm_geo_lane<L>(c, d, rx, ry, rz, lane, gmask, ng) : 0.0;
         return (1.0 - photo) + c.geo_w * geo;
     };
-    const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
-    const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
     float dcur = c.depth[idx];
     float ncur[3] = {c.normal[idx], c.normal[HW + idx], c.normal[2 * HW + idx]};
     double best, sc, ph;
     unsigned long long changed = 0;
+    if (PHASE == 1) {
+        best = c.pbest[t];
+        sc = c.psc[t];
+        changed = pflag >> 1;
+        pm_trials(c, c.pstate[t], dcur, ncur, best, sc, changed, cost);
+        if (lane != 0) return;
+        c.depth[idx] = dcur;
+        c.normal[idx] = ncur[0];
+        c.normal[HW + idx] = ncur[1];
+        c.normal[2 * HW + idx] = ncur[2];
+        pm_finish(c, idx, dcur, best, sc, changed);
+        return;
+    }
+    const int offy[8] = {-1, 1, 0, 0, -5, 5, 0, 0};
+    const int offx[8] = {0, 0, -1, 1, 0, 0, -5, 5};
     const double cached = c.cost_cache ? c.cost_cache[idx] : __longlong_as_double(0x7ff8000000000000LL);
     if (isfinite(dcur) && cached == cached) {
         best = cached;
@@ -841,57 +1022,54 @@ __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const 
             ++changed;
         }
     }
-    if (isfinite(dcur)) {
-        // the 8 draws of the two trials: lane k computes draw k (mod L), the group shares them
-        double mine[8 / L > 0 ? 8 / L : 1];
-#pragma unroll
-        for (int r0 = 0; r0 < 8; r0 += L) mine[r0 / L] = r0 + lane < 8 ? pm_uniform(c.seed, c.it, idx, r0 + lane) : 0.0;
-        auto draw = [&](int k) { return __shfl_sync(gmask, mine[k / L], k % L, L); };
-        for (int tr = 0; tr < 2; ++tr) {
-            const double u0 = draw(4 * tr + 0);
-            const double u1 = draw(4 * tr + 1);
-            const double u2 = draw(4 * tr + 2);
-            const double u3 = draw(4 * tr + 3);
-            const double dp = (double)dcur * (1.0 + c.dd_scale * (2.0 * u0 - 1.0));
-            double nb[3];
-            nb[0] = (double)ncur[0] + c.nn_scale * (2.0 * u1 - 1.0);
-            nb[1] = (double)ncur[1] + c.nn_scale * (2.0 * u2 - 1.0);
-            nb[2] = (double)ncur[2] + c.nn_scale * (2.0 * u3 - 1.0);
-            const double nn = sqrt(nb[0] * nb[0] + nb[1] * nb[1] + nb[2] * nb[2]);
-            if (nn < 1e-9 || dp < c.dmin || dp > c.dmax) continue;
-            nb[0] = nb[0] / nn;
-            nb[1] = nb[1] / nn;
-            nb[2] = nb[2] / nn;
-            const double cst = cost(dp, nb, ph);
-            if (cst < best) {
-                best = cst;
-                sc = ph;
-                dcur = (float)dp;
-                ncur[0] = (float)nb[0]; ncur[1] = (float)nb[1]; ncur[2] = (float)nb[2];
-                ++changed;
-            }
-        }
-    }
     if (lane != 0) return;
-    if (c.cost_cache) {
-        const bool keep = changed == 0 && isfinite(dcur);
-        c.cost_cache[idx] = keep ? best : __longlong_as_double(0x7ff8000000000000LL);
-        if (keep) c.score_cache[idx] = sc;
+    if (changed) {
+        c.depth[idx] = dcur;
+        c.normal[idx] = ncur[0];
+        c.normal[HW + idx] = ncur[1];
+        c.normal[2 * HW + idx] = ncur[2];
     }
-    c.depth[idx] = dcur;
-    c.normal[idx] = ncur[0];
-    c.normal[HW + idx] = ncur[1];
-    c.normal[2 * HW + idx] = ncur[2];
-    c.score[idx] = (float)sc;
-    if (changed && c.changed) atomicAdd(c.changed, changed);
+    c.pbest[t] = best;
+    c.psc[t] = sc;
+    c.flags[t] = (unsigned char)((isfinite(dcur) ? 1u : 0u) | ((unsigned)changed << 1));
 }
 
 }  // namespace mvs
 
 using namespace mvs;
 
-extern "C" double mvs_pm_uniform(uint32_t seed, int32_t it, int64_t pixel, int32_t draw) {
-    return pm_uniform(seed, it, pixel, draw);
+namespace {
+
+// Powers of the xorshift32 step matrix: P[j] = A^(2^j), j < 64 (A^(2^j) for the stream jumps).
+struct StreamTables {
+    Gf2 P[64];
+    PMJump J;   // J.t[j] = A^(8 * 2^j) = P[j + 3]
+};
+
+Gf2 gf2_mul(const Gf2& a, const Gf2& b) {   // (a b) e_i = a (b e_i)
+    Gf2 m;
+    for (int i = 0; i < 32; ++i) m.col[i] = gf2_apply(a, b.col[i]);
+    return m;
+}
+
+const StreamTables& stream_tables() {
+    static const StreamTables T = [] {
+        StreamTables t;
+        for (int i = 0; i < 32; ++i) t.P[0].col[i] = xs_step(1u << i);   // the step is linear
+        for (int j = 1; j < 64; ++j) t.P[j] = gf2_mul(t.P[j - 1], t.P[j - 1]);
+        for (int j = 0; j < 32; ++j) t.J.t[j] = t.P[j + 3];
+        return t;
+    }();
+    return T;
+}
+
+}  // namespace
+
+extern "C" uint32_t mvs_pm_stream_advance(uint32_t state, uint64_t n) {
+    const StreamTables& T = stream_tables();
+    for (int j = 0; n != 0; ++j, n >>= 1)
+        if (n & 1u) state = gf2_apply(T.P[j], state);
+    return state;
 }
 
 extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
@@ -905,12 +1083,13 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     if (a->H == 0 || a->W == 0 || a->iters <= 0) return MVS_OK;
     if (!a->ref || !a->ray || !a->Cr || !a->par || !a->depth || !a->normal || !a->score || !a->active)
         return fail(MVS_ERR_VALUE, "pm_refine: null pointer");
+    if ((long long)a->H * ((a->W + 1) / 2) >= (1LL << 31))
+        return fail(MVS_ERR_VALUE, "pm_refine: image of %d x %d pixels is too large", a->W, a->H);
     PMParams p;
     memset(&p, 0, sizeof(p));
     p.H = a->H; p.W = a->W; p.S = a->S; p.r = a->r; p.step = a->step; p.top_k = a->top_k;
     p.cr0 = a->Cr[0]; p.cr1 = a->Cr[1]; p.cr2 = a->Cr[2];
     p.geo_w = a->geo_w; p.geo_tol = a->geo_tol; p.dmin = a->dmin; p.dmax = a->dmax;
-    p.seed = a->seed | 1u;
     p.ref = a->ref; p.ray = a->ray; p.depth = a->depth; p.normal = a->normal; p.score = a->score;
     p.active = a->active;
     p.changed = reinterpret_cast<unsigned long long*>(a->changed);
@@ -939,17 +1118,31 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
             for (int i = 0; i < 3; ++i) p.bsrc[3 * s + i] = q[3 * i] * e0 + q[3 * i + 1] * e1 + q[3 * i + 2] * e2;
         }
     }
-    void* cache = nullptr;
-    if (a->iters > 1) {   // the cache pays off from the second iteration on
-        if (cudaMallocAsync(&cache, (size_t)HW * 2 * sizeof(double), st) == cudaSuccess) {
-            cudaMemsetAsync(cache, 0xFF, (size_t)HW * sizeof(double), st);   // all-ones = NaN: recompute
-            p.cost_cache = reinterpret_cast<double*>(cache);
-            p.score_cache = p.cost_cache + HW;
-        } else {
-            cudaGetLastError();   // no cache: every visit recomputes (same results)
-        }
+    // scratch, one stream-ordered allocation: per pass pixel the propagation result, its flag and
+    // stream state; per scan block a count; the stream state (two words, alternating passes);
+    // from the second iteration on, the per-pixel cost cache
+    const long long n = (long long)a->H * ((a->W + 1) / 2);
+    const int nb = (int)((n + PM_SCAN_BLOCK - 1) / PM_SCAN_BLOCK);
+    const bool use_cache = a->iters > 1;
+    auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
+    const size_t o_best = 0, o_sc = o_best + up(n * 8), o_state = o_sc + up(n * 8), o_flags = o_state + up(n * 4);
+    const size_t o_bsum = o_flags + up(n), o_rng = o_bsum + up((size_t)nb * 4), o_cache = o_rng + 256;
+    const size_t bytes = o_cache + (use_cache ? (size_t)HW * 2 * sizeof(double) : 0);
+    char* scratch = nullptr;
+    MVS_CUDA(cudaMallocAsync((void**)&scratch, bytes, st), "pm_refine: scratch");
+    p.pbest = reinterpret_cast<double*>(scratch + o_best);
+    p.psc = reinterpret_cast<double*>(scratch + o_sc);
+    unsigned* pstate = reinterpret_cast<unsigned*>(scratch + o_state);
+    p.pstate = pstate;
+    p.flags = reinterpret_cast<unsigned char*>(scratch + o_flags);
+    unsigned* bsum = reinterpret_cast<unsigned*>(scratch + o_bsum);
+    unsigned* rng = reinterpret_cast<unsigned*>(scratch + o_rng);
+    if (use_cache) {
+        p.cost_cache = reinterpret_cast<double*>(scratch + o_cache);
+        p.score_cache = p.cost_cache + HW;
+        cudaMemsetAsync(p.cost_cache, 0xFF, (size_t)HW * sizeof(double), st);   // all-ones = NaN: recompute
     }
-    const long long nthreads = (long long)a->H * ((a->W + 1) / 2);
+    const PMJump& J = stream_tables().J;
     // float32 lanes: one per source; a block holds as many pixel groups as its staged windows fit
     const int lanes = a->S <= 4 ? 4 : (a->S <= 8 ? 8 : 16);
     const int side = pm_side(a->r, a->step);
@@ -958,36 +1151,49 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     while (groups > 1 && (size_t)groups * win_bytes > 96 * 1024) groups >>= 1;
     const int block = fast ? groups * lanes : 128;
     const size_t smem = fast ? (size_t)groups * win_bytes : 0;
-    void (*lane_kernel)(PMParams) = nullptr;
+    void (*lane_kernel[2])(PMParams) = {nullptr, nullptr};
+    mvs_status status = MVS_OK;
     if (fast) {
-#define PM_PICK(LN)                                                              \
-    lane_kernel = side == 7 ? pm_lane_kernel<LN, 7> : side == 5 ? pm_lane_kernel<LN, 5> \
-                                                    : pm_lane_kernel<LN, 0>;
-        if (lanes == 4) { PM_PICK(4) } else if (lanes == 8) { PM_PICK(8) } else { PM_PICK(16) }
+#define PM_PICK(LN, PH)                                                                           \
+    lane_kernel[PH] = side == 7 ? pm_lane_kernel<LN, 7, PH> : side == 5 ? pm_lane_kernel<LN, 5, PH> \
+                                                            : pm_lane_kernel<LN, 0, PH>;
+        if (lanes == 4) { PM_PICK(4, 0) PM_PICK(4, 1) }
+        else if (lanes == 8) { PM_PICK(8, 0) PM_PICK(8, 1) }
+        else { PM_PICK(16, 0) PM_PICK(16, 1) }
 #undef PM_PICK
-        MVS_CUDA(cudaFuncSetAttribute(lane_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                 "pm_refine: shared-memory carve-out");
+        for (int ph = 0; ph < 2 && status == MVS_OK; ++ph) {
+            if (cudaFuncSetAttribute(lane_kernel[ph], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+                status = fail(MVS_ERR_CUDA, "pm_refine: shared-memory carve-out");
+        }
     }
-    const unsigned grid = fast ? (unsigned)((nthreads * lanes + block - 1) / block) : (unsigned)((nthreads + 127) / 128);
-    for (int it = 0; it < a->iters; ++it) {
+    const unsigned grid = fast ? (unsigned)((n * lanes + block - 1) / block) : (unsigned)((n + 127) / 128);
+    if (status == MVS_OK) {
+        pm_rng_init_kernel<<<1, 1, 0, st>>>(rng, a->rng_state, a->seed | 1u);
+        status = check_launch("pm_refine: stream start");
+    }
+    int cur = 0;
+    for (int it = 0; it < a->iters && status == MVS_OK; ++it) {
         const int git = a->it0 + it;
         p.it = git;
         p.dd_scale = 0.05 / (double)(git + 1);
         p.nn_scale = 0.3 / (double)(git + 1);
-        for (int colour = 0; colour < 2; ++colour) {
+        for (int colour = 0; colour < 2 && status == MVS_OK; ++colour) {
             p.colour = colour;
-            if (!fast) {
-                pm_kernel<<<grid, 128, 0, st>>>(p);
-            } else {
-                lane_kernel<<<grid, block, smem, st>>>(p);
-            }
-            mvs_status ks = check_launch("pm_refine kernel");
-            if (ks != MVS_OK) {
-                if (cache) cudaFreeAsync(cache, st);
-                return ks;
-            }
+            if (fast) lane_kernel[0]<<<grid, block, smem, st>>>(p);
+            else pm_kernel<0><<<grid, 128, 0, st>>>(p);
+            pm_count_kernel<<<nb, PM_SCAN_BLOCK, 0, st>>>(p.flags, n, bsum);
+            pm_scan_kernel<<<1, PM_SCAN_BLOCK, 0, st>>>(bsum, nb, rng, cur, cur ^ 1, J);
+            pm_state_kernel<<<nb, PM_SCAN_BLOCK, 0, st>>>(p.flags, n, bsum, rng, cur, J, pstate);
+            if (fast) lane_kernel[1]<<<grid, block, smem, st>>>(p);
+            else pm_kernel<1><<<grid, 128, 0, st>>>(p);
+            cur ^= 1;
+            status = check_launch("pm_refine kernels");
         }
     }
-    if (cache) cudaFreeAsync(cache, st);
-    return MVS_OK;
+    if (status == MVS_OK && a->rng_state) {
+        if (cudaMemcpyAsync(a->rng_state, rng + cur, sizeof(unsigned), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            status = fail(MVS_ERR_CUDA, "pm_refine: stream state copy");
+    }
+    cudaFreeAsync(scratch, st);
+    return status;
 }

@@ -1,7 +1,9 @@
 // Plane-sweep kernels of one view: the tiled sweep (engine in sweep_tile.cuh), the ordered
 // plane-chunk merge and the sub-hypothesis parabola (finalize), plus their C-ABI entry points.
+#define MVS_SWEEP_TMA_UNIT 1   // this unit instantiates the TMA kernels and owns their fault counter
 #include "sweep_tile.cuh"
 
+#include <atomic>
 #include <cudaTypedefs.h>
 #include <mutex>
 
@@ -183,8 +185,12 @@ mvs_status validate_sweep(const mvs_sweep_args* a) {
 }
 
 // Fills the plane-invariant part of the kernel parameters (sources, geometry, state pointers).
+// try_wait iterations of the sweep's bounded TMA wait (mvs_set_wait_limit; tests only lower it)
+static std::atomic<unsigned> g_wait_limit{MVS_WAIT_LIMIT_DEFAULT};
+
 mvs_status fill_params(const mvs_sweep_args* a, SweepParams& p) {
     memset(&p, 0, sizeof(p));
+    p.wait_limit = g_wait_limit.load(std::memory_order_relaxed);
     p.H = a->H;
     p.W = a->W;
     p.n_src = a->n_src;
@@ -372,6 +378,10 @@ extern "C" mvs_status mvs_sweep_finalize(int32_t H, int32_t W, const mvs_hyp* hy
     finalize_kernel<<<(unsigned)((HW + 255) / 256), 256, 0, reinterpret_cast<cudaStream_t>(stream)>>>(
         H, W, hyp->kind, hyp->n, hyp->t0, a, hyp->step, stride, p0, p1, best, s_prev_best, s_next_best, idx, depth);
     return check_launch("finalize kernel");
+}
+
+extern "C" uint32_t mvs_set_wait_limit(uint32_t iterations) {
+    return g_wait_limit.exchange(iterations);
 }
 
 extern "C" mvs_status mvs_device_faults(uint32_t* count) {

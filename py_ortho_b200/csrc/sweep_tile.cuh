@@ -56,7 +56,7 @@ struct SweepParams {
     int hyp_kind, t0;
     int r, nchunks;
     int fresh;                         // 1: start from the initial state instead of loading it
-    int pad_;
+    unsigned wait_limit;               // try_wait iterations of the TMA tile wait
     long long map_stride;
     const float* ref;
     const float* mu;
@@ -404,9 +404,11 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 }
 
 // ---- float64 window sums (MVS_PREC_FP64_SUMS): the reference's arithmetic for the sums
-// (_sweep.h:85-178): horizontal window sums of J, J^2 and J I accumulated in float64 (products of
-// float32 values are exact there) and stored rounded to float32, as the reference stores its hs
-// rows; vertical sums, moments, variance and NCC in float64, the NCC rounded to float32 once.
+// (_sweep.h:85-178): the products J J and J I formed in float32 (float times float, as there),
+// horizontal window sums accumulated in float64 - the new column added, then the old one
+// subtracted - and stored rounded to float32, as the reference stores its hs rows; vertical sums
+// in float64 (add, then subtract), the moments scaled by 1 / k^2 and divided by the scaled count,
+// the count gate, variance and NCC in float64 (om_sw_ncc_row), the NCC rounded to float32 once.
 // On bright low-texture windows, where the NCC divides by sd_ref * sd_src ~ 1e-3, float32 running
 // sums differ from the reference by up to ~1e-3; these track it to the last float32 bit or so.
 
@@ -418,7 +420,7 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
     const int sg = tid / HR, hy = tid - sg * HR;
     const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
     const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
-    float v[NIN], jz[NIN], iz[NIN];
+    float v[NIN], jz[NIN], q2[NIN], q3[NIN];
 #pragma unroll
     for (int q = 0; q < NIN / 4; ++q) {
         const float4 a = jr[q], b = ir[q];
@@ -433,7 +435,8 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
                 v[t] = ok ? 1.f : 0.f;
             }
             jz[t] = x;
-            iz[t] = iv[u];
+            q2[t] = __fmul_rn(x, x);
+            q3[t] = __fmul_rn(x, iv[u]);
         }
     }
     float a0 = 0.f;                       // counts are small integers: exact in float32
@@ -441,10 +444,9 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
 #pragma unroll
     for (int t = RA - R; t <= RA + R; ++t) {
         if constexpr (WITHV) a0 = __fadd_rn(a0, v[t]);
-        const double j = jz[t];
-        a1 = __dadd_rn(a1, j);
-        a2 = __fma_rn(j, j, a2);
-        a3 = __fma_rn(j, (double)iz[t], a3);
+        a1 = __dadd_rn(a1, (double)jz[t]);
+        a2 = __dadd_rn(a2, (double)q2[t]);
+        a3 = __dadd_rn(a3, (double)q3[t]);
     }
     float4* row = sH + hy * TW + P * sg;
     const int kx = (sg + hy) & 7;
@@ -453,10 +455,9 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
         if (j > 0) {
             const int tn = RA + R + j, to = RA - R + j - 1;
             if constexpr (WITHV) a0 = __fadd_rn(a0, __fsub_rn(v[tn], v[to]));
-            const double jn = jz[tn], jo = jz[to];
-            a1 = __dsub_rn(__dadd_rn(a1, jn), jo);
-            a2 = __fma_rn(-jo, jo, __fma_rn(jn, jn, a2));
-            a3 = __fma_rn(-jo, (double)iz[to], __fma_rn(jn, (double)iz[tn], a3));
+            a1 = __dsub_rn(__dadd_rn(a1, (double)jz[tn]), (double)jz[to]);
+            a2 = __dsub_rn(__dadd_rn(a2, (double)q2[tn]), (double)q2[to]);
+            a3 = __dsub_rn(__dadd_rn(a3, (double)q3[tn]), (double)q3[to]);
         }
         row[j ^ kx] = make_float4(a0, (float)a1, (float)a2, (float)a3);
     }
@@ -467,7 +468,7 @@ template <int R, int KMAX, bool WITHV>
 __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const float* mu, const float* sdv,
                                           float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
     constexpr int K = 2 * R + 1;
-    const float k2 = (float)(K * K);
+    const double kkd = 1.0 / (double)(K * K);
     static_assert(ROWS % 8 == 0, "stage C rows must start on a multiple of 8");
     int sw[8];
 #pragma unroll
@@ -494,11 +495,12 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
             cji = __dsub_rn(__dadd_rn(cji, (double)hn.w), (double)ho.w);
         }
         float ncc;
-        if (WITHV && cv * 10.f <= 9.f * k2) {
+        const double cov = __dmul_rn(WITHV ? (double)cv : (double)(K * K), kkd);
+        if (cov <= 0.9) {
             ncc = -1.f;
         } else {
-            const double n = WITHV ? (double)cv : (double)k2;
-            const double mj = __ddiv_rn(cj, n), m2 = __ddiv_rn(cjj, n), mij = __ddiv_rn(cji, n);
+            const double mj = __ddiv_rn(__dmul_rn(cj, kkd), cov), m2 = __ddiv_rn(__dmul_rn(cjj, kkd), cov);
+            const double mij = __ddiv_rn(__dmul_rn(cji, kkd), cov);
             const double var = __dsub_rn(m2, __dmul_rn(mj, mj));
             const double sdj = var > 1e-6 ? __dsqrt_rn(var) : 1e-3;
             double x = __ddiv_rn(__dsub_rn(mij, __dmul_rn((double)mu[j], mj)), __dmul_rn((double)sdv[j], sdj));
@@ -523,9 +525,15 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
 // (tx - RA, ty - R): x is a multiple of 4 floats (16 bytes), rows outside the image read as 0,
 // as the per-thread loads give.
 
-// sweeps whose reference-tile copy did not complete within the bounded wait (read and cleared
-// by mvs_device_faults)
+// Tiles whose reference-tile copy did not complete within the bounded wait (read and cleared by
+// mvs_device_faults). The counter exists in the one translation unit that instantiates the TMA
+// kernels (sweep.cu defines MVS_SWEEP_TMA_UNIT before including this header); elsewhere a
+// REF_TMA instantiation does not compile, so no second, unread copy of the counter can arise.
+#ifdef MVS_SWEEP_TMA_UNIT
 static __device__ unsigned g_ref_copy_faults;
+#endif
+
+constexpr unsigned MVS_WAIT_LIMIT_DEFAULT = 1u << 20;   // try_wait iterations of a bounded wait
 
 __device__ __forceinline__ unsigned smem_addr(const void* p) {
     return (unsigned)__cvta_generic_to_shared(p);
@@ -547,9 +555,10 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// Bounded wait for phase `parity` of an mbarrier: false if it did not complete.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-    for (unsigned it = 0; it < (1u << 20); ++it) {
+// Bounded wait for phase `parity` of an mbarrier: false if it did not complete within `limit`
+// try_wait iterations.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned limit) {
+    for (unsigned it = 0; it < limit; ++it) {
         unsigned done;
         asm volatile(
             "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
@@ -582,6 +591,9 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
     __syncthreads();   // a previous tile of a persistent CTA is done with shared memory
     bool tma = false;
     __shared__ __align__(8) unsigned long long s_ref_bar;
+#ifndef MVS_SWEEP_TMA_UNIT
+    static_assert(!REF_TMA, "REF_TMA kernels are instantiated in sweep.cu only (it owns the fault counter)");
+#else
     if constexpr (REF_TMA) {
         tma = p.ref_tma != 0;
         if (tma && tid == 0) {
@@ -589,6 +601,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             tma_load_2d(sI, &p.ref_map, tx - RA, ty - R, &s_ref_bar, (unsigned)(HR * JP * sizeof(float)));
         }
     }
+#endif
     for (int e = tid; e < HR * JP; e += NT) {
         if (!tma) {
             const int hy = e / JP, hc = e - hy * JP;
@@ -631,17 +644,25 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
     const int nlist = bottom ? nsrc - kk : kk;
     // every halo sample lies inside the reference image (interior tile)
     const bool tile_inside = tx - R >= 0 && ty - R >= 0 && tx + TW + R <= W && ty + TH + R <= H;
+#ifdef MVS_SWEEP_TMA_UNIT
     if constexpr (REF_TMA) {
         if (tma) {
             __syncthreads();   // the barrier's initialisation is visible to every thread
-            const bool arrived = mbar_wait_bounded(&s_ref_bar, 0);
-            // a copy that never completed: count it and leave the tile's state untouched
+            const bool arrived = mbar_wait_bounded(&s_ref_bar, 0, p.wait_limit);
+            // a copy that did not complete in time: count it and leave the tile's state untouched.
+            // Before the CTA (and its shared memory) goes, wait once more, with the default
+            // bound, for the copy that may still be in flight into that memory.
             if (__syncthreads_or(!arrived)) {
-                if (tid == 0) atomicAdd(&g_ref_copy_faults, 1u);
+                if (tid == 0) {
+                    atomicAdd(&g_ref_copy_faults, 1u);
+                    mbar_wait_bounded(&s_ref_bar, 0, MVS_WAIT_LIMIT_DEFAULT);
+                }
+                __syncthreads();
                 return;
             }
         }
     }
+#endif
 
     for (int i = pa; i < pb; ++i) {
         float topk[ROWS][KMAX];

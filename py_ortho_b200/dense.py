@@ -228,15 +228,19 @@ PM_PRECISIONS = {"fp64": 0, "fp32": 1}     # mvs_pm_precision
 
 def pm_refine(ref, ray, Cr, srcs: Sequence, src_depths: Sequence, par, depth, normal, score, active, r: int,
               step: int, top_k: int, geo_w: float, geo_tol: float, iters: int, dmin: float, dmax: float,
-              seed: int, it0: int = 0, precision: str = "fp64") -> int:
+              seed: int, it0: int = 0, precision: str = "fp64", rng_state=None) -> int:
     """Slanted-plane PatchMatch repair (reference: _dense.pyx:566-666); depth / normal / score are
-    updated in place; returns the number of accepted hypothesis changes. Random trials use
-    counter-based draws (mvs_pm_uniform) instead of one sequential xorshift stream.
+    updated in place; returns the number of accepted hypothesis changes. The random trials draw
+    from the reference's own xorshift32 stream (started at seed | 1), in its raster order.
 
     precision: "fp64" evaluates the reference's float64 cost operation for operation (bit-identical
-    to a sequential evaluation with the same draws); "fp32" evaluates the windows in float32 from
-    one float64-composed homography per candidate and source (costs within ~1e-6 of float64;
-    near-ties may be decided differently)."""
+    to the reference's pm_refine); "fp32" evaluates the windows in float32 from one
+    float64-composed homography per candidate and source (costs within ~1e-6 of float64; near-ties
+    may be decided differently).
+
+    rng_state: None, or a 1-element int32 CUDA tensor holding the stream state (initialise it
+    with stream_start(seed)); the call starts there and leaves the state after its draws, so a
+    job split over calls (it0 = iterations done) matches one call."""
     if precision not in PM_PRECISIONS:
         raise ValueError(f"pm_refine: precision must be one of {sorted(PM_PRECISIONS)}")
     S = len(srcs)
@@ -281,6 +285,11 @@ def pm_refine(ref, ray, Cr, srcs: Sequence, src_depths: Sequence, par, depth, no
         a.seed = int(seed) & 0xFFFFFFFF
         a.it0 = int(it0)
         a.changed = changed.data_ptr()
+        if rng_state is not None:
+            if not (isinstance(rng_state, torch.Tensor) and rng_state.is_cuda and rng_state.numel() == 1
+                    and rng_state.dtype == torch.int32 and rng_state.device == ref_t.device):
+                raise ValueError("pm_refine: rng_state must be a 1-element int32 tensor on the image's device")
+            a.rng_state = rng_state.data_ptr()
         L.check(L.load().mvs_pm_refine(C_addr(a), L.stream_handle()), "pm_refine")
         out = int(changed.item())
         D.close()
@@ -289,6 +298,13 @@ def pm_refine(ref, ray, Cr, srcs: Sequence, src_depths: Sequence, par, depth, no
         D.back = []
 
 
-def pm_uniform(seed: int, it: int, pixel: int, draw: int) -> float:
-    """The counter-based draw used by pm_refine."""
-    return float(L.load().mvs_pm_uniform(seed & 0xFFFFFFFF, it, pixel, draw))
+def stream_start(seed: int, device=None) -> torch.Tensor:
+    """A PatchMatch stream state for pm_refine(rng_state=...): seed | 1, as the reference starts."""
+    v = (int(seed) | 1) & 0xFFFFFFFF
+    return torch.tensor([v - (1 << 32) if v >= 1 << 31 else v], dtype=torch.int32,
+                        device=device if device is not None else L.require_cuda())
+
+
+def stream_advance(state: int, n: int) -> int:
+    """The xorshift32 state after n steps of the PatchMatch stream (GF(2) jump-ahead, host)."""
+    return int(L.load().mvs_pm_stream_advance(int(state) & 0xFFFFFFFF, int(n)))

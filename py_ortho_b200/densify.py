@@ -9,6 +9,7 @@ Reference: densify.py:57-81 (DepthOptions), :94-130 (_box, _norm, _half), :133-1
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass
 
 import numpy as np
@@ -16,7 +17,7 @@ import torch
 
 from . import _lib as L
 from . import fast
-from .dense import Hypotheses, finalize, new_state, sweep
+from .dense import C_addr, Hypotheses, finalize, new_state, sweep
 
 
 @dataclass
@@ -194,71 +195,70 @@ def _sweep_maps(ref, cam_r, srcs, cams_s, inv_list, opt, ray, block: int = 32):
     return depth, state[0], sd
 
 
-# ------------------------------------------------------------------ per-image geometry (host)
+# ------------------------------------------------------------------ tie-point priors of a view
+def _cam_row(R, C, f, k1, k2, k3, cx, cy) -> np.ndarray:
+    return np.ascontiguousarray(np.r_[np.asarray(R, np.float64).ravel(), np.asarray(C, np.float64), f, k1, k2, k3,
+                                      cx, cy], np.float64)
+
+
 def _depth_range(rec, k):
-    """Depth search range of image k from all tie points in its view (densify.py:208-230)."""
-    it = rec.intr[rec.cam_group[k]]
-    xc = (rec.X - rec.C[k]) @ rec.R[k].T
-    z = xc[:, 2]
-    with np.errstate(divide="ignore", invalid="ignore"):
-        u = it.f * xc[:, 0] / z + it.cx
-        v = it.f * xc[:, 1] / z + it.cy
-    inside = (z > 0) & (u >= 0) & (v >= 0) & (u < it.width) & (v < it.height)
-    d = z[inside]
-    if len(d) < 10:
+    """Depth search range of view k (densify.py:208-230). Every tie point of the block is
+    projected into the view on the device (mvs_tie_depths); from the depths of those that land
+    inside, the 1st-99th percentile interval is stretched far enough to reach the block's lowest
+    ground (the 0.5th percentile of tie-point heights) along the optical axis - whose downward
+    cosine is floored at 0.2 - and then padded: 20 % of the span each side, plus 1 m below the
+    near end (kept above 30 % of it) and 2 m beyond the far end. None below 10 points."""
+    intr = rec.intr[rec.cam_group[k]]
+    X = np.ascontiguousarray(rec.X, np.float64)
+    if X.shape[0] == 0:
         return None
-    lo, hi = np.percentile(d, [1, 99])
-    zlow = float(np.percentile(rec.X[:, 2], 0.5))
-    axis_down = max(-float(rec.R[k][2, 2]), 0.2)
-    hi = max(hi, (float(rec.C[k][2]) - zlow) / axis_down)
-    span = hi - lo
-    return max(0.3 * lo, lo - 0.2 * span - 1.0), hi + 0.2 * span + 2.0
+    row = _cam_row(rec.R[k], rec.C[k], intr.f, 0.0, 0.0, 0.0, intr.cx, intr.cy)
+    d_X = torch.from_numpy(X).to(L.require_cuda())
+    z = torch.empty(X.shape[0], dtype=torch.float64, device=d_X.device)
+    L.check(L.load().mvs_tie_depths(X.shape[0], d_X.data_ptr(), L.host_ptr(row), int(intr.width), int(intr.height),
+                                    z.data_ptr(), L.stream_handle()), "tie_depths")
+    z = z.cpu().numpy()
+    seen = z[~np.isnan(z)]
+    if seen.size < 10:
+        return None
+    near, far = np.percentile(seen, [1, 99])
+    ground = float(np.percentile(X[:, 2], 0.5))
+    cos_down = max(-float(rec.R[k][2, 2]), 0.2)
+    far = max(far, (float(rec.C[k][2]) - ground) / cos_down)
+    span = far - near
+    return max(0.3 * near, near - 0.2 * span - 1.0), far + 0.2 * span + 2.0
 
 
-def _depth_band(rec, k, cam, shape, rng, block: int = 32, margin: float = 1.0):
-    """Per-pixel inverse-depth band from image k's own tie points (densify.py:233-274)."""
+def _band_maps(rec, k, cam, shape, rng, nd: int, block: int = 32, margin: float = 1.0):
+    """The coarse sweep's linear hypothesis maps over the per-pixel inverse-depth band that view
+    k's own tie points give (densify.py:233-274, 409-411), computed on the device
+    (mvs_depth_band). Returns device tensors (base, step, inv_hi) at `shape`."""
     H, W = shape
-    m = rec.obs_cam == k
-    lo_g, hi_g = rng
-    inv_lo = np.full((H, W), 1.0 / hi_g, np.float32)
-    inv_hi = np.full((H, W), 1.0 / lo_g, np.float32)
-    if m.sum() < 50:
-        return inv_lo, inv_hi
-    xc = (rec.X[rec.obs_pt[m]] - cam.C) @ cam.R.T
-    ok = xc[:, 2] > 0
-    u, v = cam.project_cam(xc[ok, 0], xc[ok, 1], xc[ok, 2])
-    z = xc[ok, 2]
-    gh, gw = -(-H // block), -(-W // block)
-    bi = (np.clip(v, 0, H - 1) // block).astype(int) * gw + (np.clip(u, 0, W - 1) // block).astype(int)
-    inb = (u >= 0) & (v >= 0) & (u < W) & (v < H)
-    bi, z = bi[inb], z[inb]
-    zlo = np.full(gh * gw, np.inf)
-    zhi = np.full(gh * gw, -np.inf)
-    cnt = np.bincount(bi, minlength=gh * gw)
-    np.minimum.at(zlo, bi, z)
-    np.maximum.at(zhi, bi, z)
-    ok_b = (cnt >= 5).reshape(gh, gw)
-    zlo, zhi = zlo.reshape(gh, gw), zhi.reshape(gh, gw)
-    pl = np.pad(np.where(ok_b, zlo, np.inf), 1, constant_values=np.inf)
-    ph = np.pad(np.where(ok_b, zhi, -np.inf), 1, constant_values=-np.inf)
-    lo3 = np.min([pl[1 + dy:gh + 1 + dy, 1 + dx:gw + 1 + dx] for dy in (-1, 0, 1) for dx in (-1, 0, 1)], 0)
-    hi3 = np.max([ph[1 + dy:gh + 1 + dy, 1 + dx:gw + 1 + dx] for dy in (-1, 0, 1) for dx in (-1, 0, 1)], 0)
-    has = ok_b & np.isfinite(lo3) & np.isfinite(hi3)
-    pad = margin + 0.05 * (hi3 - lo3)
-    lo_b = np.where(has, np.clip(lo3 - pad, lo_g, hi_g), lo_g)
-    hi_b = np.where(has, np.clip(hi3 + pad, lo_g, hi_g), hi_g)
-    lo_px = np.repeat(np.repeat(lo_b, block, 0), block, 1)[:H, :W]
-    hi_px = np.repeat(np.repeat(hi_b, block, 0), block, 1)[:H, :W]
-    return (1.0 / hi_px).astype(np.float32), (1.0 / np.maximum(lo_px, 1e-6)).astype(np.float32)
+    dev = L.require_cuda()
+    pts = np.ascontiguousarray(rec.X[rec.obs_pt[rec.obs_cam == k]], np.float64)
+    d_pts = torch.from_numpy(pts).to(dev) if len(pts) >= L.BAND_MIN_POINTS else None
+    out = [torch.empty((H, W), dtype=torch.float32, device=dev) for _ in range(3)]
+    row = _cam_row(cam.R, cam.C, cam.f, cam.k1, cam.k2, cam.k3, cam.cx, cam.cy)
+    a = L.DepthBandArgs()
+    a.H, a.W, a.block, a.n_pts = int(H), int(W), int(block), int(len(pts))
+    a.X = 0 if d_pts is None else d_pts.data_ptr()
+    a.cam = L.host_ptr(row)
+    a.lo, a.hi, a.margin = float(rng[0]), float(rng[1]), float(margin)
+    a.nd = int(nd)
+    a.base, a.step, a.inv_hi = (t.data_ptr() for t in out)
+    L.check(L.load().mvs_depth_band(C_addr(a), L.stream_handle()), "depth_band")
+    return tuple(out)
 
 
 def _num_depths(rec, k, nbrs_k, rng, f_coarse, base: int) -> int:
-    """Coarse-sweep hypothesis count (densify.py:277-284)."""
+    """Coarse-sweep hypothesis count (densify.py:277-284): about one hypothesis per pixel of
+    disparity that the median baseline to the neighbours spans over the depth range at the
+    coarse focal length, kept within [base, 3 base]."""
     if not nbrs_k:
         return base
-    B = float(np.median([np.linalg.norm(rec.C[k] - rec.C[j]) for j in nbrs_k]))
-    disp = f_coarse * B * (1.0 / rng[0] - 1.0 / rng[1])
-    return int(np.clip(np.ceil(disp), base, 3 * base))
+    baseline = float(np.median([np.linalg.norm(rec.C[k] - rec.C[j]) for j in nbrs_k]))
+    span_px = f_coarse * baseline * (1.0 / rng[0] - 1.0 / rng[1])
+    return int(min(max(math.ceil(span_px), base), 3 * base))
 
 
 def _upsample2(a: torch.Tensor, H: int, W: int) -> torch.Tensor:
@@ -286,6 +286,7 @@ def depth_map(k, nbrs, rec, views, opt: DepthOptions):
         return None
     depth, score, low = out
     torch.cuda.current_stream().synchronize()
+    L.check_device_faults()
     return depth.cpu().numpy(), score.cpu().numpy(), low.cpu().numpy()
 
 
@@ -315,9 +316,7 @@ def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
         rays.append(fast.half(rays[-1][:, :2 * h, :2 * w].contiguous()))
     nd = _num_depths(rec, k, nbrs, rng, pyr_c[lv].f, opt.num_depths)
     shape = tuple(pyr_r[lv].shape)
-    inv_lo, inv_hi = _depth_band(rec, k, pyr_c[lv], shape, rng, block=max(8, shape[1] // 16))
-    step = ((inv_hi - inv_lo) / max(nd - 1, 1)).astype(np.float32)
-    base_t, step_t = _dev(inv_lo), _dev(step)
+    base_t, step_t, _ = _band_maps(rec, k, pyr_c[lv], shape, rng, nd, block=max(8, shape[1] // 16))
     d, _, _, _ = sweep_device(pyr_r[lv], pyr_c[lv], pyr_s[lv], pyr_cs[lv], Hypotheses.linear(base_t, step_t, nd),
                               opt, rays[lv], precision=_per_pixel_precision(opt))
     dstep = step_t / 2

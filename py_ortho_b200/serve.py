@@ -28,7 +28,7 @@ import torch
 
 from . import _lib as L
 from . import fast
-from .dense import Hypotheses, new_state, sweep_args
+from .dense import Hypotheses, new_state, stream_start, sweep_args
 
 
 @dataclass
@@ -272,8 +272,11 @@ class DepthServer:
             j.pm_normal = torch.from_numpy(tilted_normals(H, W, int(rng.integers(1 << 30)))).to(self.dev, non_blocking=True)
             j.pm_score = torch.zeros((H, W), dtype=torch.float32, device=self.dev)
             j.pm_active = torch.ones((H, W), dtype=torch.uint8, device=self.dev)
+            # the job's random stream stays on the device between its one-iteration steps
+            j.pm_rng = stream_start(req.seed, self.dev)
         j.pm, j.pm_keep = pm_args(j.ref, j.pm_ray, req.ref_cam, j.srcs, req.src_cams, j.pm_depth, j.pm_normal,
                                   j.pm_score, j.pm_active, req, iters=1)
+        j.pm.rng_state = j.pm_rng.data_ptr()
         j.pm_started = False
 
 

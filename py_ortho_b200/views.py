@@ -337,6 +337,7 @@ def densify_views(rec, views, opt: DepthOptions, nbrs: Optional[List[List[int]]]
         score, low = extra[k]
         D, ch, na = repair(k, maps, score, low, views, nbrs[k], rec, settings, opt)
         torch.cuda.current_stream().synchronize()
+        L.check_device_faults()      # a sweep tile of pass 1 or 2 that gave up raises here
         return D.cpu().numpy(), ch, na
 
     return run_passes(N, nbrs, costs, shapes, pass1, pass2, group=group, device=dev)

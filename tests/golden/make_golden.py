@@ -3,6 +3,7 @@
 source into oracle/_ref) on seeded inputs.
 
 Run where the reference tree exists:  make -C oracle ref && python tests/golden/make_golden.py
+(optionally followed by the names of the cases to regenerate, e.g. ``pm_case8``).
 The fixtures travel with the repository; nothing at test time needs the reference.
 
 Fixtures (each .npz holds the inputs and the reference outputs):
@@ -17,6 +18,8 @@ Fixtures (each .npz holds the inputs and the reference outputs):
                      best-to-second hypothesis score gap
   helpers.npz      - _fast.box_zero_mean, hyp_linear, hyp_refine, depth_view, densify._rays_world
   pm_case.npz      - _dense.pm_refine (the reference's xorshift draws) on a small case
+  pm_case8.npz     - _dense.pm_refine on a rendered 192 x 144 scene with 8 sources, 7 x 7 window,
+                     2 iterations (uint8 images; the grey inputs are (g - 128) / 64)
   depth_map.npz    - densify.depth_map end to end (3-level pyramid, tie-point depth band, coarse
                      sweep + 2 refinement levels) on a rendered scene with a synthetic
                      reconstruction (tie points on the terrain, their in-image observations)
@@ -247,6 +250,36 @@ def pm_case(R):
                             args["dmax"], args["seed"])
     out.update({"depth": depth, "normal": normal, "score": score, "changed": np.array(ch)})
     np.savez_compressed(os.path.join(HERE, "pm_case.npz"), **out)
+
+
+def pm_case8(R):
+    from py_ortho_b200 import scene as S
+    W, H = 192, 144
+    sc = S.make_scene("c2", seed=21, width=W, height=H)
+    ref_u8 = np.ascontiguousarray(sc.ref)
+    src_u8 = np.stack([np.ascontiguousarray(s) for s in sc.srcs[:8]])
+    ref = sc.grey(ref_u8)
+    srcs = [sc.grey(s) for s in src_u8]
+    ray = O.rays_world((H, W), sc.ref_cam)
+    par = np.array([c.row() for c in sc.src_cams[:8]], np.float64)
+    rng = np.random.default_rng(23)
+    depth = (sc.depth_true * (1 + rng.normal(0, 0.01, (H, W)))).astype(np.float32)
+    depth[rng.random((H, W)) < 0.01] = np.nan
+    normal = S.tilted_normals(H, W, 29)
+    score = np.zeros((H, W), np.float32)
+    active = (rng.random((H, W)) < 0.8).astype(np.uint8)
+    zr = float(sc.ref_cam.C[2])
+    args = dict(r=3, step=1, top_k=2, geo_w=0.0, geo_tol=0.02, iters=2, dmin=zr - 40.0, dmax=zr + 5.0, seed=4242)
+    out = {"ref_u8": ref_u8, "src_u8": src_u8, "ray": ray, "par": par, "Cr": np.asarray(sc.ref_cam.C, np.float64),
+           "depth0": depth.copy(), "normal0": normal.copy(), "active": active,
+           "args": np.array([args["r"], args["step"], args["top_k"], args["iters"], args["seed"]]),
+           "fargs": np.array([args["geo_w"], args["geo_tol"], args["dmin"], args["dmax"]])}
+    ch = R._dense.pm_refine(ref, ray, out["Cr"], srcs, [None] * 8, par, depth, normal, score, active, args["r"],
+                            args["step"], args["top_k"], args["geo_w"], args["geo_tol"], args["iters"], args["dmin"],
+                            args["dmax"], args["seed"])
+    out.update({"depth": depth, "normal": normal, "score": score, "changed": np.array(ch)})
+    print("pm_case8: changes", ch)
+    np.savez_compressed(os.path.join(HERE, "pm_case8.npz"), **out)
 
 
 def depth_map_case(D):
@@ -542,15 +575,13 @@ def main():
     R = O.reference()
     if D is None or R is None:
         raise SystemExit("the reference is not available here: build oracle/_ref first (make -C oracle ref)")
-    sweep_cases(R)
-    sweep_e2e(D)
-    scene_small(D)
-    helpers(D, R)
-    pm_case(R)
-    depth_map_case(D)
-    views_case(D)
-    fuse_case(D)
-    height_case()
+    cases = {"sweep_cases": lambda: sweep_cases(R), "sweep_e2e": lambda: sweep_e2e(D),
+             "scene_small": lambda: scene_small(D), "helpers": lambda: helpers(D, R), "pm_case": lambda: pm_case(R),
+             "pm_case8": lambda: pm_case8(R), "depth_map": lambda: depth_map_case(D),
+             "views_case": lambda: views_case(D), "fuse_case": lambda: fuse_case(D), "height_case": height_case}
+    wanted = sys.argv[1:] or list(cases)
+    for name in wanted:
+        cases[name]()
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -41,7 +41,8 @@ def test_ctypes_structs_match_the_c_layout(tmp_path):
     structs = {"mvs_hyp": L.Hyp, "mvs_sweep_args": L.SweepArgs, "mvs_pm_args": L.PMArgs,
                "mvs_batch_job": L.BatchJob, "mvs_batch_tuning": L.BatchTuning,
                "mvs_consistency_args": L.ConsArgs, "mvs_fuse_args": L.FuseArgs,
-               "mvs_sample_view_args": L.SampleViewArgs, "mvs_height_score_args": L.HeightScoreArgs}
+               "mvs_sample_view_args": L.SampleViewArgs, "mvs_height_score_args": L.HeightScoreArgs,
+               "mvs_depth_band_args": L.DepthBandArgs}
     lines = ['#include <stdio.h>', '#include <stddef.h>', f'#include "{HEADER}"', "int main(void) {"]
     for cname, py in structs.items():
         lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
@@ -145,10 +146,17 @@ def test_python_layer_validates_before_touching_the_device():
     assert dense.pm_refine(None, None, None, [], [], None, None, None, None, None, 1, 1, 2, 0.0, 1.0, 1, 0, 1, 0) == 0
 
 
-def test_counter_draws_agree_with_the_oracle():
+def test_stream_jump_ahead_matches_sequential_steps():
+    """mvs_pm_stream_advance (GF(2) matrix powers, the jumps mvs_pm_refine's trials take) against
+    the reference's xorshift32 stepped one draw at a time."""
     from oracle import oracle as O
     lib = _lib().load()
-    for seed in (1, 99, 4294967295):
-        for pix in (0, 5, 10 ** 9):
-            for d in range(8):
-                assert lib.mvs_pm_uniform(seed, 2, pix, d) == O.pm_uniform(seed, 2, pix, d)
+    for state in (1, 12345 | 1, 0xDEADBEEF, 0xFFFFFFFF):
+        for n in (0, 1, 2, 7, 8, 31, 64, 1000, 4099):
+            assert lib.mvs_pm_stream_advance(state, n) == O.xorshift_steps(state, n)
+    # composition over a large jump: (a + b) steps = b steps after a steps
+    s = 0x2545F491
+    for a, b in ((1 << 20, 12345), (3 << 27, 1 << 31), ((1 << 40) + 5, 777)):
+        assert lib.mvs_pm_stream_advance(lib.mvs_pm_stream_advance(s, a), b) == lib.mvs_pm_stream_advance(s, a + b)
+    # the period of a full-period xorshift32 is 2^32 - 1
+    assert lib.mvs_pm_stream_advance(s, (1 << 32) - 1) == s

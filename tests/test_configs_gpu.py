@@ -1,0 +1,117 @@
+"""Parity at the measured configurations, through the C ABI, against the oracle (the reference's
+per-hypothesis kernel restated in C and pinned bit for bit to the reference's own kernel):
+
+* C1 in full: 640 x 480, 4 sources, 128 inverse-depth planes over [35, 55] m, 5 x 5 window,
+  best-2 of 4 (the whole view, every pixel);
+* C2, the benchmark's step: 4000 x 3000, 8 sources, 256 planes over [60, 90] m, 7 x 7 window;
+  the device sweeps the whole view and three row bands of it are checked against the oracle
+  (each band swept by the oracle on a crop with an r-row halo and the full view's window
+  statistics, so its rows see exactly the full view's inputs).
+
+The bar is the one the depth-map path is specified by: winner index exact wherever the best-to-
+second score gap exceeds 1e-3, depth within 0.1 % relative everywhere else (flipped pixels
+included)."""
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as O
+from tests_support import SCORE_ABS, check_parity, gap_of
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
+
+
+def _device_sweep(ref, srcs, sc, planes, r, top_k, precision=None):
+    from py_ortho_b200 import _lib as L
+    from py_ortho_b200 import dense, fast, scene as S
+    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+    ref_d = ref if isinstance(ref, torch.Tensor) else _dev(ref)
+    mu, sd = fast.ref_stats(ref_d, r)
+    hyp = dense.Hypotheses.planes_inv(planes)
+    srcs_d = [s if isinstance(s, torch.Tensor) else _dev(s) for s in srcs]
+    st = dense.sweep(ref_d, mu, sd, None, srcs_d, geo, hyp, r, top_k, ref_cam=sc.ref_cam.row(),
+                     precision=L.PREC_FP32 if precision is None else precision)
+    depth = dense.finalize(hyp, st)
+    torch.cuda.synchronize()
+    return st, depth, mu, sd, geo
+
+
+def _score_report(best, ref_best, same):
+    e = np.abs(best.astype(np.float64) - ref_best)[same]
+    return {"score_abs_max": float(e.max()), "score_abs_q999": float(np.quantile(e, 0.999)),
+            "score_over_bar": int((e > SCORE_ABS).sum())}
+
+
+def test_c1_full_view_parity():
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c1", seed=0, device="cuda")
+    ref = sc.grey(sc.ref)
+    srcs = [sc.grey(s) for s in sc.srcs]
+    H, W = ref.shape
+    assert (H, W, len(srcs)) == (480, 640, 4)
+    planes = S.plane_list(35.0, 55.0, 128)
+    r, top_k = 2, 2
+    st, depth, _, _, geo = _device_sweep(ref, srcs, sc, planes, r, top_k)
+    ray = O.rays_world((H, W), sc.ref_cam)
+    full = O.sweep(ref, srcs, ray, geo, [np.full((H, W), p, np.float32) for p in planes], r, top_k, keep_scores=True)
+    idx, d, best = st[4].cpu().numpy(), depth.cpu().numpy(), st[0].cpu().numpy()
+    rep = check_parity(idx, d, None, full["idx"], full["depth"], None, gap_of(full["scores"]), "C1 640x480",
+                       flip_depth_frac=1e-4)
+    rep.update(_score_report(best, full["best"], idx == full["idx"]))
+    print("C1 parity:", rep)
+    assert rep["decided"] > 0.5 * H * W
+
+
+def _oracle_rows(ref, mu, sd, srcs, ray, geo, planes, r, top_k, y0, y1):
+    """The oracle's sweep of rows [y0, y1) of a large view: a crop with an r-row halo on each side
+    and the full view's window statistics."""
+    H, W = ref.shape
+    a, b = max(0, y0 - r), min(H, y1 + r)
+    c = lambda x: np.ascontiguousarray(x[a:b])
+    cref, cmu, csd, cray = c(ref), c(mu), c(sd), np.ascontiguousarray(ray[:, a:b])
+    h = b - a
+    best, prev, spb, snb, idx = O.init_state(h, W)
+    top1 = np.full((h, W), -np.inf, np.float32)
+    top2 = np.full((h, W), -np.inf, np.float32)
+    for i, p in enumerate(planes):
+        O.sweep_hypothesis(cref, cmu, csd, srcs, cray, geo, np.full((h, W), p, np.float32), r, top_k, i, best, prev,
+                           spb, snb, idx)
+        top2 = np.where(prev > top1, top1, np.maximum(top2, prev))
+        top1 = np.maximum(top1, prev)
+    inv0 = np.full((h, W), planes[0], np.float32)
+    inv1 = np.full((h, W), planes[1], np.float32)
+    depth = O.finalize(best, spb, snb, idx, inv0, inv1, len(planes))
+    rows = slice(y0 - a, y1 - a)
+    return {"idx": idx[rows], "depth": depth[rows], "best": best[rows], "gap": (top1 - top2)[rows]}
+
+
+def test_c2_bench_step_row_bands_parity():
+    from py_ortho_b200 import scene as S
+    sc = S.make_scene("c2", seed=0, device="cuda")
+    ref = sc.grey(sc.ref)
+    srcs = [sc.grey(s) for s in sc.srcs]
+    H, W = ref.shape
+    assert (H, W, len(srcs)) == (3000, 4000, 8)
+    planes = S.plane_list(60.0, 90.0, 256)
+    r, top_k = 3, 2
+    st, depth, mu, sd, geo = _device_sweep(ref, srcs, sc, planes, r, top_k)
+    mu, sd = mu.cpu().numpy(), sd.cpu().numpy()
+    ray = O.rays_world((H, W), sc.ref_cam)
+    idx, d, best = st[4].cpu().numpy(), depth.cpu().numpy(), st[0].cpu().numpy()
+    bands = [(0, 24), (1488, 1512), (2976, 3000)]        # top edge, middle, bottom edge
+    with ThreadPoolExecutor(len(bands)) as ex:
+        outs = list(ex.map(lambda b: _oracle_rows(ref, mu, sd, srcs, ray, geo, planes, r, top_k, *b), bands))
+    reps = []
+    for (y0, y1), o in zip(bands, outs):
+        rep = check_parity(idx[y0:y1], d[y0:y1], None, o["idx"], o["depth"], None, o["gap"], f"C2 rows {y0}-{y1}",
+                           flip_depth_frac=1e-4)
+        rep.update(_score_report(best[y0:y1], o["best"], idx[y0:y1] == o["idx"]))
+        reps.append(rep)
+        assert rep["decided"] > 0.5 * (y1 - y0) * W
+    print("C2 band parity:", reps)

@@ -102,26 +102,44 @@ def test_oracle_pm_matches_reference_fixture():
     sdeps = [None, z["sdep1"], None]
     depth, normal, score = z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()
     ch = O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], depth, normal, score, z["active"], r, step,
-                     top_k, geo_w, geo_tol, iters, dmin, dmax, seed, rng=0)
+                     top_k, geo_w, geo_tol, iters, dmin, dmax, seed)
     assert ch == int(z["changed"])
     assert same_bits(depth, z["depth"]) and same_bits(normal, z["normal"]) and same_bits(score, z["score"])
 
 
-def test_oracle_pm_counter_rng_is_deterministic():
+def test_oracle_pm_matches_reference_rendered_8_sources():
+    """The oracle against the reference's own pm_refine on a rendered 8-source scene (7 x 7, 2
+    iterations, 1 % holes, 80 % active)."""
+    z = golden("pm_case8.npz")
+    r, step, top_k, iters, seed = (int(v) for v in z["args"])
+    geo_w, geo_tol, dmin, dmax = (float(v) for v in z["fargs"])
+    grey = lambda u8: ((u8.astype(np.float32) - np.float32(128)) / np.float32(64)).astype(np.float32)
+    srcs = [grey(u) for u in z["src_u8"]]
+    st = [z["depth0"].copy(), z["normal0"].copy(), np.zeros(z["depth0"].shape, np.float32)]
+    ch = O.pm_refine(grey(z["ref_u8"]), z["ray"], z["Cr"], srcs, [None] * len(srcs), z["par"], *st, z["active"], r,
+                     step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed)
+    assert ch == int(z["changed"])
+    for a, b in zip(st, (z["depth"], z["normal"], z["score"])):
+        assert same_bits(a, b)
+
+
+def test_oracle_pm_stream_carries_across_calls():
+    """Iterations split over calls, with the stream state carried, equal one call (the resumable
+    form the device takes with mvs_pm_args.rng_state)."""
     z = golden("pm_case.npz")
     r, step, top_k, iters, seed = (int(v) for v in z["args"])
     geo_w, geo_tol, dmin, dmax = (float(v) for v in z["fargs"])
     srcs = [z[f"src{j}"] for j in range(3)]
-    outs = []
-    for _ in range(2):
-        depth, normal, score = z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()
-        ch = O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, [None, z["sdep1"], None], z["par"], depth, normal, score,
-                         z["active"], r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed, rng=1)
-        outs.append((ch, depth, normal, score))
-    assert outs[0][0] == outs[1][0] and outs[0][0] > 0
-    assert all(same_bits(a, b) for a, b in zip(outs[0][1:], outs[1][1:]))
-    u = [O.pm_uniform(seed, 0, p, d) for p in range(50) for d in range(8)]
-    assert 0.0 <= min(u) and max(u) < 1.0 and 0.4 < np.mean(u) < 0.6
+    sdeps = [None, z["sdep1"], None]
+    one = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
+    c1 = O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *one, z["active"], r, step, top_k, geo_w,
+                     geo_tol, 3, dmin, dmax, seed)
+    two = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
+    st = np.array([seed | 1], np.uint32)
+    c2 = sum(O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *two, z["active"], r, step, top_k,
+                         geo_w, geo_tol, 1, dmin, dmax, seed, it0=it, state=st) for it in range(3))
+    assert c1 == c2 > 0
+    assert all(same_bits(a, b) for a, b in zip(one, two))
 
 
 def test_oracle_fp64_agrees_with_float32_where_decided():
@@ -152,22 +170,3 @@ def test_oracle_matches_live_reference_kernels():
             O.sweep_hypothesis(ref, mu, sd, srcs, ray, geo, inv, r, top_k, i, *s1)
             R._dense.sweep_hypothesis(ref, mu, sd, srcs, ray, geo, np.ascontiguousarray(inv), r, top_k, i, *s2)
         assert all(same_bits(a, b) for a, b in zip(s1, s2))
-
-
-def test_depth_map_host_geometry_matches_reference():
-    """The driver's host-side helpers (depth range, tie-point band, hypothesis count) restated in
-    py_ortho_b200.densify give the reference's values on the depth_map fixture."""
-    from types import SimpleNamespace
-    from py_ortho_b200 import densify as Dn
-    z = golden("depth_map.npz")
-    f, cx, cy, w, h = z["intr"]
-    rec = SimpleNamespace(intr=[SimpleNamespace(f=f, cx=cx, cy=cy, width=int(w), height=int(h))],
-                          cam_group=np.zeros(len(z["C"]), np.int32), X=z["X"], C=z["C"], R=z["R"],
-                          obs_cam=z["obs_cam"], obs_pt=z["obs_pt"])
-    rng = Dn._depth_range(rec, 0)
-    assert np.array_equal(np.array(rng), z["range"])
-    cam = Dn._Cam(z["R"][0], z["C"][0], float(f), 0.0, 0.0, float(cx), float(cy), int(w), int(h))
-    cam2 = cam.scaled(0.5, 160, 120).scaled(0.5, 80, 60)
-    lo, hi = Dn._depth_band(rec, 0, cam2, (60, 80), rng, block=max(8, 80 // 16))
-    assert same_bits(lo, z["band_lo"]) and same_bits(hi, z["band_hi"])
-    assert Dn._num_depths(rec, 0, [1, 2, 3, 4], rng, cam2.f, int(z["opt"][1])) == int(z["nd"])

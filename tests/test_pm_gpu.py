@@ -1,6 +1,8 @@
-"""PatchMatch on the device against the oracle. With the same counter-based draws the device
-kernel (float64, no contraction) and the sequential oracle are bit-identical: parallel red-black
-updates equal the reference's raster order because every neighbour has the other colour."""
+"""PatchMatch on the device against the reference and the oracle. The device draws from the
+reference's own xorshift32 stream (per colour pass: a prefix count of the drawing pixels in raster
+order and a GF(2) jump to each pixel's offset), so the float64 kernel (no contraction) is
+bit-identical to the reference's pm_refine: parallel red-black updates equal the reference's
+raster order because every neighbour has the other colour."""
 import numpy as np
 import pytest
 import torch
@@ -19,16 +21,9 @@ def _case():
     return z, srcs, [None, z["sdep1"], None], (r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed)
 
 
-def test_counter_draws_match_the_oracle():
-    from py_ortho_b200 import dense
-    for seed in (1, 12345, 2654435761):
-        for it in (0, 3):
-            for pix in (0, 17, 123456789):
-                for d in range(8):
-                    assert dense.pm_uniform(seed, it, pix, d) == O.pm_uniform(seed, it, pix, d)
-
-
-def test_pm_refine_bit_exact_vs_oracle():
+def test_pm_refine_bit_exact_vs_reference():
+    """The reference's own pm_refine output (golden, made by its compiled kernel) and the oracle:
+    same depth, normal and score bits, same change count."""
     from py_ortho_b200 import dense
     z, srcs, sdeps, (r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed) = _case()
     a = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
@@ -36,43 +31,78 @@ def test_pm_refine_bit_exact_vs_oracle():
     ch_gpu = dense.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *a, z["active"], r, step, top_k,
                              geo_w, geo_tol, iters, dmin, dmax, seed)
     ch_cpu = O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *b, z["active"], r, step, top_k, geo_w,
-                         geo_tol, iters, dmin, dmax, seed, rng=1)
-    assert ch_gpu == ch_cpu > 0
-    for x, y in zip(a, b):
+                         geo_tol, iters, dmin, dmax, seed)
+    assert ch_gpu == ch_cpu == int(z["changed"]) > 0
+    for x, y, ref in zip(a, b, (z["depth"], z["normal"], z["score"])):
         assert same_bits(x, y)
+        assert same_bits(x, ref)
 
 
 def test_pm_refine_resumes_across_calls():
-    """Iterations split over calls (it0) give the same result as one call (resumable jobs)."""
+    """Iterations split over calls (it0, the stream state carried on the device) give the same
+    result as one call (resumable jobs)."""
     from py_ortho_b200 import dense
     z, srcs, sdeps, (r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed) = _case()
     one = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
     two = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
     c1 = dense.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *one, z["active"], r, step, top_k, geo_w,
                          geo_tol, 3, dmin, dmax, seed)
+    st = dense.stream_start(seed)
     c2 = 0
     for it in range(3):
         c2 += dense.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *two, z["active"], r, step, top_k,
-                              geo_w, geo_tol, 1, dmin, dmax, seed, it0=it)
+                              geo_w, geo_tol, 1, dmin, dmax, seed, it0=it, rng_state=st)
     assert c1 == c2
     for x, y in zip(one, two):
         assert same_bits(x, y)
+    # the state left on the device is the oracle's after the same draws
+    ost = np.array([seed | 1], np.uint32)
+    three = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
+    O.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *three, z["active"], r, step, top_k, geo_w,
+                geo_tol, 3, dmin, dmax, seed, state=ost)
+    assert int(st.cpu().numpy().view(np.uint32)[0]) == int(ost[0])
 
 
-def test_pm_refine_improves_photo_consistency_like_the_reference():
-    """Statistical agreement with the reference's own pm_refine (its xorshift stream differs):
-    both lower the mean cost on the fixture and end with similar score distributions."""
+def test_pm_refine_bit_exact_vs_reference_rendered_8_sources():
+    """A rendered 8-source scene (golden from the reference's own pm_refine: noisy depth, 1 % holes,
+    80 % active, 7 x 7 window, 2 iterations): the device result equals the reference's bits."""
     from py_ortho_b200 import dense
-    z, srcs, sdeps, (r, step, top_k, geo_w, geo_tol, iters, dmin, dmax, seed) = _case()
-    a = [z["depth0"].copy(), z["normal0"].copy(), z["score0"].copy()]
-    dense.pm_refine(z["ref"], z["ray"], z["Cr"], srcs, sdeps, z["par"], *a, z["active"], r, step, top_k, geo_w,
-                    geo_tol, iters, dmin, dmax, seed)
-    act = z["active"].astype(bool) & np.isfinite(z["ref"])
-    s_gpu, s_ref = a[2][act], z["score"][act]
-    assert abs(np.median(s_gpu) - np.median(s_ref)) < 0.05
-    d_gpu, d_ref = a[0][act], z["depth"][act]
-    fin = np.isfinite(d_gpu) & np.isfinite(d_ref)
-    assert np.median(np.abs(d_gpu[fin] - d_ref[fin]) / d_ref[fin]) < 0.01
+    z = golden("pm_case8.npz")
+    r, step, top_k, iters, seed = (int(v) for v in z["args"])
+    geo_w, geo_tol, dmin, dmax = (float(v) for v in z["fargs"])
+    grey = lambda u8: ((u8.astype(np.float32) - np.float32(128)) / np.float32(64)).astype(np.float32)
+    ref = grey(z["ref_u8"])
+    srcs = [grey(u) for u in z["src_u8"]]
+    st = [z["depth0"].copy(), z["normal0"].copy(), np.zeros(ref.shape, np.float32)]
+    ch = dense.pm_refine(ref, z["ray"], z["Cr"], srcs, [None] * len(srcs), z["par"], *st, z["active"], r, step, top_k,
+                         geo_w, geo_tol, iters, dmin, dmax, seed)
+    assert ch == int(z["changed"]) > 0
+    for x, ref_out in zip(st, (z["depth"], z["normal"], z["score"])):
+        assert same_bits(x, ref_out)
+
+
+def test_pm_fp32_against_the_reference_rendered_8_sources():
+    """The float32 mode against the reference's own result on the rendered 8-source case: the same
+    stream (which pixels draw does not depend on the cost arithmetic), so only near-ties decided
+    the other way differ. Depth within 0.1 % of the reference on >= 99.9 % of pixels."""
+    from py_ortho_b200 import dense
+    z = golden("pm_case8.npz")
+    r, step, top_k, iters, seed = (int(v) for v in z["args"])
+    geo_w, geo_tol, dmin, dmax = (float(v) for v in z["fargs"])
+    grey = lambda u8: ((u8.astype(np.float32) - np.float32(128)) / np.float32(64)).astype(np.float32)
+    ref = grey(z["ref_u8"])
+    srcs = [grey(u) for u in z["src_u8"]]
+    st = [z["depth0"].copy(), z["normal0"].copy(), np.zeros(ref.shape, np.float32)]
+    dense.pm_refine(ref, z["ray"], z["Cr"], srcs, [None] * len(srcs), z["par"], *st, z["active"], r, step, top_k,
+                    geo_w, geo_tol, iters, dmin, dmax, seed, precision="fp32")
+    d, dr = st[0].astype(np.float64), z["depth"].astype(np.float64)
+    assert np.array_equal(np.isfinite(d), np.isfinite(dr))
+    fin = np.isfinite(dr)
+    rel = np.abs(d[fin] - dr[fin]) / dr[fin]
+    print(f"fp32 PatchMatch vs reference: identical {(rel == 0).mean():.4%}, within 0.1 % {(rel <= 1e-3).mean():.4%}, "
+          f"median {np.median(rel):.1e}")
+    assert (rel <= 1e-3).mean() >= 0.999
+    assert np.median(rel) == 0.0
 
 
 def test_pm_no_sources_is_a_noop():

@@ -381,3 +381,47 @@ def test_fp64_sums_meet_the_bar_at_every_pixel_on_planes():
     job = batch.ViewJob(_dev(ref), [_dev(s) for s in srcs], sc.ref_cam, sc.src_cams, planes, r=2, top_k=2).prepare()
     with pytest.raises(NotImplementedError, match="single-view"):
         batch.Batch([job], precision=L.PREC_FP64_SUMS)
+
+
+def test_reference_tile_wait_gives_up_cleanly():
+    """The give-up path of the bounded wait for the reference tile's TMA copy, made to run out
+    without any fault: with a wait limit of 0 every tile gives up at once, counts itself, lets its
+    copy in flight land (second wait, default bound) and returns with its state untouched. The
+    count is read by mvs_device_faults (TimeoutError), the context stays usable, and with the
+    default limit back the same sweep gives the normal result."""
+    import ctypes
+    from py_ortho_b200 import _lib as L, dense, scene as S
+    from oracle import oracle as O
+    lib = L.load()
+    sc = S.make_scene("c1", seed=4, width=128, height=96)
+    ref = sc.grey(sc.ref)
+    srcs = [torch.from_numpy(sc.grey(s)).cuda() for s in sc.srcs]
+    geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+    planes = S.plane_list(35.0, 55.0, 12)
+    mu, sd = O.ref_stats(ref, 2)
+    H, W = ref.shape
+    args = (torch.from_numpy(ref).cuda(), torch.from_numpy(mu).cuda(), torch.from_numpy(sd).cuda(), None, srcs, geo,
+            dense.Hypotheses.planes_inv(planes), 2, 2)
+    lib.mvs_device_faults(None)                               # start from a clear count
+    old = lib.mvs_set_wait_limit(0)
+    try:
+        st = dense.sweep(*args, ref_cam=sc.ref_cam.row(), plane_chunks=1)
+        torch.cuda.synchronize()
+    finally:
+        assert lib.mvs_set_wait_limit(old) == 0
+    n = ctypes.c_uint32(0)
+    with pytest.raises(TimeoutError, match="gave up"):
+        L.check(lib.mvs_device_faults(ctypes.byref(n)), "device faults")
+    tiles = ((W + 63) // 64) * ((H + 31) // 32)
+    assert n.value == tiles
+    init = dense.new_state(H, W)
+    for a, b in zip(st, init):
+        assert same_bits(a.cpu().numpy(), b.cpu().numpy())
+    # the count was cleared by the read; the default limit gives the normal sweep
+    again = dense.sweep(*args, ref_cam=sc.ref_cam.row(), plane_chunks=1)
+    normal = dense.sweep(*args, ref_cam=sc.ref_cam.row(), plane_chunks=3)
+    torch.cuda.synchronize()
+    L.check(lib.mvs_device_faults(ctypes.byref(n)), "device faults")
+    assert n.value == 0
+    for a, b in zip(again, normal):
+        assert same_bits(a.cpu().numpy(), b.cpu().numpy())

@@ -50,7 +50,7 @@ def test_oracle_init_normals_and_pass2_patchmatch_match_reference():
     ray = O.rays_world((H, W), cams[k])
     N0 = O.init_normals(z[f"p{k}"], ray)
     assert same_bits(N0, z["norm_out"])
-    # the reference's pass-2 PatchMatch (its sequential xorshift draws, rng=0), geometric term on
+    # the reference's pass-2 PatchMatch (its sequential xorshift draws), geometric term on
     k = int(z["have"][0])
     nb = list(z[f"nbrs{k}"])
     r, step, top_k, iters, seed = (int(v) for v in z[f"pm{k}_args"])
@@ -62,7 +62,7 @@ def test_oracle_init_normals_and_pass2_patchmatch_match_reference():
     par = np.array([O.cam_row(cams[j]) for j in nb])
     ch = O.pm_refine(greys[k], ray, np.asarray(cams[k].C, np.float64), [greys[j] for j in nb],
                      [z[f"p{j}"] for j in nb], par, D, N, S, z[f"pm{k}_active"], r, step, top_k, gw, gt, iters,
-                     dmin, dmax, seed, rng=0)
+                     dmin, dmax, seed)
     assert ch == int(z[f"pm{k}_changed"])
     assert same_bits(D, z[f"pm{k}_depth_out"]) and same_bits(N, z[f"pm{k}_normal_out"])
     assert same_bits(S, z[f"pm{k}_score_out"])

@@ -48,9 +48,10 @@ def test_init_normals_match_reference():
     assert same_bits(_init_normals(z[f"p{k}"], ray.cpu().numpy()), z["norm_out"])
 
 
-def test_pass2_patchmatch_matches_oracle():
-    """The device repair of one view (geometric term on the neighbours' maps) against the oracle
-    with the same counter-based draws: bit-identical depth, normal, score and change count."""
+def test_pass2_patchmatch_matches_reference():
+    """The device repair of one view (geometric term on the neighbours' maps, the inputs the
+    reference's own pass 2 received) against the reference's pm_refine output and the oracle:
+    bit-identical depth, normal, score and change count (the reference's xorshift32 stream)."""
     from oracle import oracle as O
     from py_ortho_b200 import dense, fast
     z, rec, cams, greys = views_fixture()
@@ -67,13 +68,15 @@ def test_pass2_patchmatch_matches_oracle():
     S0 = z[f"s{k}"].astype(np.float32)
     Do, No, So = D0.copy(), N0.copy(), S0.copy()
     ch_o = O.pm_refine(greys[k], ray, cams[k].C, [greys[j] for j in nb], [z[f"p{j}"] for j in nb], par, Do, No, So,
-                       act, r, step, top_k, gw, gt, iters, dmin, dmax, seed, rng=1)
+                       act, r, step, top_k, gw, gt, iters, dmin, dmax, seed)
     Dg, Ng, Sg = _dev(D0), _dev(N0), _dev(S0)
     ch_g = dense.pm_refine(_dev(greys[k]), _dev(ray), cams[k].C, [_dev(greys[j]) for j in nb],
                            [_dev(z[f"p{j}"]) for j in nb], par, Dg, Ng, Sg, _dev(act), r, step, top_k, gw, gt,
                            iters, dmin, dmax, seed)
-    assert ch_g == ch_o and ch_o > 0
+    assert ch_g == ch_o == int(z[f"pm{k}_changed"]) > 0
     assert same_bits(Dg.cpu().numpy(), Do) and same_bits(Ng.cpu().numpy(), No) and same_bits(Sg.cpu().numpy(), So)
+    assert same_bits(Dg.cpu().numpy(), z[f"pm{k}_depth_out"]) and same_bits(Ng.cpu().numpy(), z[f"pm{k}_normal_out"])
+    assert same_bits(Sg.cpu().numpy(), z[f"pm{k}_score_out"])
 
 
 def test_densify_views_end_to_end_against_reference():

@@ -56,7 +56,33 @@ def test_noalloc_sweep_matches_mvs_sweep_on_two_calls_in_a_row():
         assert same_bits(x, y)
 
 
+def _pool():
+    """The device's current memory pool: the one stream-ordered allocations (cudaMallocAsync,
+    as mvs_sweep uses for its chunk records) draw from."""
+    from cuda.bindings import driver as d
+    err, dev = d.cuCtxGetDevice()
+    assert err == d.CUresult.CUDA_SUCCESS, err
+    err, pool = d.cuDeviceGetMemPool(dev)
+    assert err == d.CUresult.CUDA_SUCCESS, err
+    return d, pool
+
+
+def _pool_used_high(d, pool) -> int:
+    err, v = d.cuMemPoolGetAttribute(pool, d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH)
+    assert err == d.CUresult.CUDA_SUCCESS, err
+    return int(v)
+
+
+def _pool_reset_high(d, pool):
+    err, = d.cuMemPoolSetAttribute(pool, d.CUmemPool_attribute.CU_MEMPOOL_ATTR_USED_MEM_HIGH, d.cuuint64_t(0))
+    assert err == d.CUresult.CUDA_SUCCESS, err
+
+
 def test_noalloc_allocates_nothing_and_rejects_oversized_scratch():
+    """No allocation, shown two ways: the pool's high-water mark of memory in use (reset to zero
+    first) stays zero across noalloc calls while one mvs_sweep call with the same arguments raises
+    it - so a pooled stream-ordered allocation, which returns its memory to the pool and leaves
+    the free-memory figure unchanged, would be seen - and the device's free memory is unchanged."""
     from py_ortho_b200 import _lib as L
     dense, ref, mu, sd, srcs, geo, ref_cam, planes = _inputs()
     hyp = dense.Hypotheses.planes_inv(planes)
@@ -65,11 +91,19 @@ def test_noalloc_allocates_nothing_and_rejects_oversized_scratch():
     lib = L.load()
     L.check(lib.mvs_sweep_noalloc(ctypes.addressof(a), L.stream_handle()))   # set-up call
     torch.cuda.synchronize()
+    d, pool = _pool()
     free0 = torch.cuda.mem_get_info()[0]
+    _pool_reset_high(d, pool)
+    assert _pool_used_high(d, pool) == 0
     for _ in range(3):
         L.check(lib.mvs_sweep_noalloc(ctypes.addressof(a), L.stream_handle()))
     torch.cuda.synchronize()
+    assert _pool_used_high(d, pool) == 0
     assert torch.cuda.mem_get_info()[0] == free0
+    # the probe sees a pooled allocation: the allocating entry point, same arguments
+    L.check(lib.mvs_sweep(ctypes.addressof(a), L.stream_handle()))
+    torch.cuda.synchronize()
+    assert _pool_used_high(d, pool) >= 6 * 8 * ref.shape[0] * ref.shape[1] * 4
     # 48 chunks x 6 records x 320 x 240 floats = 88 MB > 32 MiB: a clear error, nothing launched
     big = 6 * 48 * ref.shape[0] * ref.shape[1] * 4
     assert big > CAPACITY
