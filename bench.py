@@ -50,11 +50,15 @@ def parse():
     ap.add_argument("--pm-iters", type=int, default=-1)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--mode", choices=["headline", "batch", "serve", "fuse", "height"], default="headline",
+    ap.add_argument("--mode", choices=["headline", "batch", "serve", "fuse", "height", "depthmap"], default="headline",
                     help="headline: the single-view step above; batch: 64 uneven views in one persistent "
                          "launch vs per-view launches; serve: Poisson arrivals through the continuous-batching server")
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (jobs/s)")
+    ap.add_argument("--serve-precision", choices=["fp32", "fp16"], default="fp16")
+    ap.add_argument("--no-modes", action="store_true",
+                    help="headline only: skip the batched (config 4) and served (config 5) summaries that a "
+                         "1-GPU run appends to its line")
     ap.add_argument("--seed", type=int, default=0)
     return ap.parse_args()
 
@@ -299,6 +303,8 @@ def run_ours(a):
                               prec)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(cfg, nplanes, iters, device=dev)   # sample rendered on the GPU
+    if world == 1 and a.mode == "headline" and not a.no_modes:
+        line.update(mode_summaries(a, dev))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -601,12 +607,17 @@ def view_jobs(n_jobs, cams, imgs, dev, seed, prec=None):
 
 
 def run_batch(a):
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    print(json.dumps(batch_summary(a, dev)), flush=True)
+
+
+def batch_summary(a, dev):
     """Config 4: per-view launches (plain single-view kernel) vs one persistent batched launch in
     a CUDA graph (autotuned plane chunk / CTAs per SM), FP32 and FP16 storage."""
     import torch
     from py_ortho_b200 import _lib as L, batch, dense, fast
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
     t0 = time.time()
     cfg, cams, imgs = flight(dev, a.seed)
     jobs = view_jobs(a.jobs, cams, imgs, dev, a.seed)
@@ -678,21 +689,26 @@ def run_batch(a):
             "speedup_fp16_batched_vs_plain": ms_plain / ms_16, "speedup_fp32_batched_vs_plain": ms_plain / ms_batch,
             "config": {"workload": "c4: 64 views, long side U(1200,4000) 4:3, 4-12 sources, 96-384 planes, 5x5/7x7",
                        "flight": "4x4 grid, 75 % overlap, 4000x3000, f=3600, 80 m; references are crops"}}
-    print(json.dumps(line), flush=True)
+    return line
 
 
 def run_serve(a):
+    import torch
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    print(json.dumps(serve_summary(a, dev, a.rate, a.serve_precision)), flush=True)
+
+
+def serve_summary(a, dev, rate, precision="fp32", flight_data=None):
     """Config 5: Poisson arrivals through the continuous-batching server vs the plain
     per-request path on the same trace; p50 / p99 latency and throughput."""
     import torch
     from py_ortho_b200 import serve as SV
-    dev = torch.device("cuda", 0)
-    torch.cuda.set_device(dev)
     t0 = time.time()
-    cfg, cams, imgs = flight(dev, a.seed)
+    cfg, cams, imgs = flight_data if flight_data is not None else flight(dev, a.seed)
     jobs = view_jobs(a.jobs, cams, imgs, dev, a.seed + 1)
     rng = np.random.default_rng(a.seed + 2)
-    arrivals = np.cumsum(rng.exponential(1.0 / a.rate, len(jobs)))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(jobs)))
     pm = rng.random(len(jobs)) < 0.1
 
     def trace():
@@ -708,20 +724,127 @@ def run_serve(a):
     # whole requests per step (their 96-384 planes in one chunk), oldest first within a 3e10
     # evaluation budget: measured better than 96- and 192-plane chunks in median, tail and
     # throughput on the same trace
-    srv = SV.DepthServer(hbm_budget=120e9, max_slots=64, plane_chunk=384, shared_sources=True, step_evals=3e10)
+    srv = SV.DepthServer(hbm_budget=120e9, max_slots=64, plane_chunk=384, shared_sources=True, step_evals=3e10,
+                         precision=precision)
     res_s, wall_s = SV.serve(trace(), srv, realtime=True)
     srv.close()
-    res_p, wall_p = SV.serve_plain(trace(), realtime=True)
+    res_p, wall_p = SV.serve_plain(trace(), realtime=True)          # the plain FP32 per-request kernel
     same = all(np.array_equal(x.depth, y.depth, equal_nan=True) for x, y in zip(res_s, res_p))
+    rel = []
+    for x, y in zip(res_s, res_p):
+        m = np.isfinite(x.depth) & np.isfinite(y.depth) & (y.depth > 0)
+        rel.append(np.abs(x.depth[m].astype(np.float64) - y.depth[m]) / y.depth[m])
+    rel = np.concatenate(rel) if rel else np.zeros(1)
     span_s = max(r.finished for r in res_s) - float(arrivals[0])
     span_p = max(r.finished for r in res_p) - float(arrivals[0])
     line = {"mode": "serve", "metric": "latency p50/p99 ms and ZNCC evaluations/s", "jobs": len(jobs),
-            "pm_jobs": int(pm.sum()), "rate_jobs_per_s": a.rate, "evals": evals, "setup_s": round(setup, 1),
+            "pm_jobs": int(pm.sum()), "rate_jobs_per_s": rate, "precision": precision, "evals": evals,
+            "setup_s": round(setup, 1),
             "server": dict(SV.latency_stats(res_s), throughput=evals / span_s / 1e9, steps=srv.steps),
             "plain": dict(SV.latency_stats(res_p), throughput=evals / span_p / 1e9),
-            "identical_results": bool(same), "unit_throughput": "Gpix.plane.view/s",
+            "identical_results": bool(same), "depth_rel_vs_plain_fp32_median": float(np.median(rel)),
+            "depth_rel_vs_plain_fp32_p99": float(np.percentile(rel, 99)),
+            "speedup_throughput": (evals / span_s) / (evals / span_p), "unit_throughput": "Gpix.plane.view/s",
             "config": {"workload": "c5: Poisson arrivals, c4 size/source/plane distribution, 10 % PatchMatch (4 it)",
                        "hbm_budget_gb": 120, "plane_chunk": 384, "step_evals": 3e10, "max_slots": 64}}
+    return line
+
+
+def mode_summaries(a, dev):
+    """Config 4 (64 uneven views: per-view launches vs one persistent launch in a CUDA graph, FP32
+    and FP16 storage) and config 5 (the FP16 continuous-batching server against the plain FP32
+    per-request kernel at 20 and 200 jobs/s, 10 % PatchMatch jobs), appended to a 1-GPU headline
+    line after its timed region. A failure is reported in the line instead of ending the run."""
+    import torch
+    out = {}
+    try:
+        out["c4_batched"] = batch_summary(a, dev)
+    except Exception as e:            # noqa: BLE001 - reported, the headline stands
+        out["c4_batched"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
+    try:
+        fl = flight(dev, a.seed)
+        out["c5_served"] = [serve_summary(a, dev, rate, "fp16", fl) for rate in (20.0, 200.0)]
+    except Exception as e:            # noqa: BLE001
+        out["c5_served"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_depthmap(a):
+    """The drop-in driver itself (densify.depth_map, densify.py:373-437) on the benchmark's view:
+    4000 x 3000 reference, 8 sources, 7 x 7 window, default DepthOptions otherwise; tie points are
+    20000 seeded terrain points with their in-image observations. One step = depth_map_device end
+    to end: pyramids, ray grids, the tie-point depth range and band (device), the coarse sweep over
+    the per-pixel band at 1/4 resolution (MVS_HYP_LINEAR, float64 ray sampler) and two refinement
+    levels of 2 refine_steps + 1 hypotheses (MVS_HYP_REFINE). CUDA events around the step."""
+    import torch
+    from types import SimpleNamespace
+    from py_ortho_b200 import densify as Dn, scene as S
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    cfg = S.CONFIGS["c2"]
+    W, H = a.width or cfg.width, a.height or cfg.height
+    sc = S.make_scene(cfg, seed=a.seed, device=dev, width=W, height=H)
+    cams = [sc.ref_cam] + list(sc.src_cams)
+    greys = [sc.grey(sc.ref)] + [sc.grey(x) for x in sc.srcs]
+    rng = np.random.default_rng(a.seed)
+    t = sc.terrain
+    hx, hy = 0.5 * W * cfg.altitude / sc.ref_cam.f, 0.5 * H * cfg.altitude / sc.ref_cam.f
+    xs, ys = rng.uniform(-hx, hx, 20000), rng.uniform(-hy, hy, 20000)
+    zs = S._height(torch.from_numpy(xs), torch.from_numpy(ys), torch.from_numpy(t.hills),
+                   torch.from_numpy(t.boxes)).numpy()
+    X = np.column_stack([xs, ys, zs])
+    obs_cam, obs_pt = [], []
+    for k, c in enumerate(cams):
+        xc = (X - c.C) @ c.R.T
+        u = c.f * xc[:, 0] / xc[:, 2] + c.cx
+        v = c.f * xc[:, 1] / xc[:, 2] + c.cy
+        ok = (xc[:, 2] > 0) & (u >= 0) & (v >= 0) & (u < c.w) & (v < c.h)
+        obs_cam.append(np.full(ok.sum(), k, np.int32))
+        obs_pt.append(np.flatnonzero(ok).astype(np.int32))
+    intr = [SimpleNamespace(f=cams[0].f, cx=cams[0].cx, cy=cams[0].cy, width=W, height=H, k1=0.0, k2=0.0, k3=0.0)]
+    rec = SimpleNamespace(intr=intr, cam_group=np.zeros(len(cams), np.int32), X=X, C=np.array([c.C for c in cams]),
+                          R=np.array([c.R for c in cams]), obs_cam=np.concatenate(obs_cam),
+                          obs_pt=np.concatenate(obs_pt))
+    dcams = [Dn._Cam(c.R, c.C, float(c.f), 0.0, 0.0, float(c.cx), float(c.cy), c.w, c.h, 0.0) for c in cams]
+    views = lambda k: (greys[k], None, dcams[k])         # host images, as densify's ImageCache hands them
+    opt = Dn.DepthOptions()
+    opt.window = cfg.radius
+    nbrs = list(range(1, len(cams)))
+    step = lambda: Dn.depth_map_device(0, nbrs, rec, views, opt)
+    for _ in range(max(1, a.warmup)):
+        step()
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(a.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        depth, score, low = step()
+        e1.record()
+        e1.synchronize()
+        ts.append(e0.elapsed_time(e1))
+    L_check = __import__("py_ortho_b200._lib", fromlist=["x"])
+    L_check.check_device_faults()
+    rng_ = Dn._depth_range(rec, 0)
+    h4, w4 = H // 4, W // 4
+    nd = Dn._num_depths(rec, 0, nbrs, rng_, dcams[0].scaled(0.25, w4, h4).f, opt.num_depths)
+    ns = len(nbrs)
+    nref = 2 * opt.refine_steps + 1
+    evals = h4 * w4 * nd * ns + ((H // 2) * (W // 2) + H * W) * nref * ns
+    ms = statistics.median(ts)
+    d = depth.cpu().numpy()
+    fin = np.isfinite(d)
+    rel = np.abs(d[fin] - sc.depth_true[fin]) / sc.depth_true[fin]
+    line = {"mode": "depthmap", "metric": "ZNCC evaluations/s (pixel x hypothesis x view), depth_map end to end",
+            "unit": "Gpix.plane.view/s", "value": evals / (ms / 1e3) / 1e9, "ms_per_step": ms, "ms": ts,
+            "evals_per_step": evals, "coarse_hypotheses": nd,
+            "depth_vs_truth": {"finite": float(fin.mean()), "median_rel": float(np.median(rel)),
+                               "within_1pct": float((rel < 0.01).mean())},
+            "config": {"workload": f"densify.depth_map on c2 {W}x{H}, {ns} sources, window {2 * cfg.radius + 1}, "
+                                   f"num_depths {opt.num_depths}, refine_steps {opt.refine_steps}, 20000 tie points",
+                       "path": "MVS_HYP_LINEAR coarse band + 2 x MVS_HYP_REFINE, float64 ray sampler; the "
+                               "step includes the host -> device copies of the 9 grey images"}}
     print(json.dumps(line), flush=True)
 
 
@@ -840,6 +963,8 @@ def main():
         run_fuse(a)
     elif a.mode == "height":
         run_height(a)
+    elif a.mode == "depthmap":
+        run_depthmap(a)
     elif a.mode == "serve":
         run_serve(a)
     else:

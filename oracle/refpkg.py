@@ -14,8 +14,11 @@ import os
 import sys
 import types
 
-REF_SRC = os.environ.get("MVS_REFERENCE_SRC", "/root/reference/orthomosaic")
 HERE = os.path.dirname(os.path.abspath(__file__))
+# the reference's package sources: $MVS_REFERENCE_SRC, else the `reference` tree beside this
+# repository's root
+REF_SRC = os.environ.get("MVS_REFERENCE_SRC",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "orthomosaic"))
 
 
 def load_densify():

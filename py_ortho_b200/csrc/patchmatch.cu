@@ -517,6 +517,11 @@ __global__ void pm_rng_init_kernel(unsigned* rng, const unsigned* from, unsigned
 // Float32 costs differ from the float64 ones by ~1e-7 (measured 99.9th percentile 2e-6), so the
 // strict '<' can decide near-ties differently; the float64 mode is the bit-exact reference.
 
+// samples of a window row unrolled in the unchecked window sums (0: the whole row)
+#ifndef PM_ROW_UNROLL
+#define PM_ROW_UNROLL 0
+#endif
+constexpr int kRowUnroll = PM_ROW_UNROLL;   // (a pragma argument is not macro-expanded)
 #ifndef PM_LANE_MIN_BLOCKS
 #define PM_LANE_MIN_BLOCKS 3
 #endif
@@ -556,7 +561,7 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
     const int NW = NSIDE > 0 ? NSIDE * NSIDE : nw;
 #pragma unroll 1
     for (int e0 = 0; e0 < NW; e0 += side)
-#pragma unroll((NSIDE > 0 && !CHECKED) ? NSIDE : 1)
+#pragma unroll((NSIDE > 0 && !CHECKED) ? (kRowUnroll > 0 ? kRowUnroll : NSIDE) : 1)
     for (int e = e0; e < e0 + side; ++e) {
         const float4 w = win[e];
         const float cq = fmaf(C[0], w.x, fmaf(C[1], w.y, fmaf(C[2], w.z, c0)));

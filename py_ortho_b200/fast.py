@@ -138,9 +138,9 @@ def half(g):
     return _out(out, host)
 
 
-def to_fp16(img: torch.Tensor) -> torch.Tensor:
+def to_fp16(img: torch.Tensor, stream=None) -> torch.Tensor:
     """float32 device image -> FP16 storage copy (round to nearest) for MVS_PREC_FP16 sweeps."""
     t = img.contiguous()
     out = torch.empty(t.shape, dtype=torch.float16, device=t.device)
-    L.check(L.load().mvs_to_fp16(t.numel(), t.data_ptr(), out.data_ptr(), L.stream_handle()), "to_fp16")
+    L.check(L.load().mvs_to_fp16(t.numel(), t.data_ptr(), out.data_ptr(), L.stream_handle(stream)), "to_fp16")
     return out

@@ -10,7 +10,15 @@ state and PatchMatch state resident on the device until it completes. Each sched
      budget allows, all their tiles - in one persistent launch (mvs_server_step), merging each
      chunk into its job's state in hypothesis order;
   3. finalises jobs whose last chunk ran, and advances PatchMatch-phase jobs by one iteration;
-  4. returns finished jobs' depth (and normal / score) to the host and frees their slot.
+     PatchMatch runs on a pool of its own streams (one per job, ordered after the job's finalize
+     by an event), so it overlaps the next sweep steps and other jobs' PatchMatch;
+  4. returns finished jobs' depth (and normal / score) to the host and frees their slot (a
+     PatchMatch job's copies are queued on its stream and collected once its event completes,
+     without blocking the step).
+
+Precision "fp16" stores the sources in FP16 for the sweep (one converted copy per source tensor,
+shared by the jobs that use it; FP32 window sums), as MVS_PREC_FP16; PatchMatch reads the float32
+sources.
 
 A job's arithmetic does not depend on which other jobs share its steps (fixed chunk boundaries,
 ordered merge, same tile engine as the single-view path), so its result equals the plain
@@ -109,7 +117,8 @@ def admissions(footprints, free_slots: int, used: float, budget: float):
 
 
 class _Job:
-    def __init__(self, req: DepthRequest, slot: int, dev, stream, plane_chunk: int):
+    def __init__(self, req: DepthRequest, slot: int, dev, stream, plane_chunk: int, precision: int = L.PREC_FP32,
+                 half=None):
         self.req, self.slot = req, slot
         H, W = req.ref.shape
         self.H, self.W = H, W
@@ -125,9 +134,12 @@ class _Job:
             self.state = new_state(H, W, dev)
             self.rec = torch.empty((6, H, W), dtype=torch.float32, device=dev)
             self.depth = torch.empty((H, W), dtype=torch.float32, device=dev)
+            # the sweep's sources: FP16 copies (shared per source tensor) in the FP16 form
+            self.sweep_srcs = [half(s) for s in self.srcs] if precision == L.PREC_FP16 else self.srcs
         self.hyp = Hypotheses.planes_inv(req.planes_inv)
-        self.args, self.keep = sweep_args(self.ref, self.mu, self.sd, None, self.srcs, _geo(req.ref_cam, req.src_cams),
-                                          fast.cam_row(req.ref_cam), self.hyp, req.r, req.top_k, self.state)
+        self.args, self.keep = sweep_args(self.ref, self.mu, self.sd, None, self.sweep_srcs,
+                                          _geo(req.ref_cam, req.src_cams), fast.cam_row(req.ref_cam), self.hyp, req.r,
+                                          req.top_k, self.state, precision=precision)
         self.nchunks = -(-len(req.planes_inv) // plane_chunk)
         self.next_chunk = 0
         self.pm_done = 0
@@ -140,9 +152,15 @@ class DepthServer:
 
     def __init__(self, hbm_budget: float = 120e9, max_slots: int = 64, plane_chunk: int = 32,
                  max_items: int = 1 << 20, max_radius: int = 3, shared_sources: bool = False,
-                 step_evals: float = 2.5e10):
+                 step_evals: float = 2.5e10, precision: str = "fp32", pm_streams: int = 4):
+        if precision not in ("fp32", "fp16"):
+            raise ValueError("server: precision must be 'fp32' or 'fp16'")
         self.dev = L.require_cuda()
         self.stream = torch.cuda.Stream(self.dev)
+        self.pm_streams = [torch.cuda.Stream(self.dev) for _ in range(max(1, pm_streams))]
+        self._pm_next = 0
+        self.precision = L.PREC_FP16 if precision == "fp16" else L.PREC_FP32
+        self._half: dict = {}          # source tensor address -> (source, FP16 copy, jobs using it)
         self.budget = float(hbm_budget)
         self.max_slots = max_slots
         self.plane_chunk = plane_chunk
@@ -152,7 +170,7 @@ class DepthServer:
         # without time-slicing every resident job)
         self.step_evals = float(step_evals)
         h = ctypes.c_void_p()
-        L.check(L.load().mvs_server_create(max_slots, max_items, max_radius, L.PREC_FP32, ctypes.byref(h)),
+        L.check(L.load().mvs_server_create(max_slots, max_items, max_radius, self.precision, ctypes.byref(h)),
                 "server_create")
         self._h = h
         self.free_slots = list(range(max_slots))[::-1]
@@ -181,6 +199,26 @@ class DepthServer:
             raise ValueError("server: window radius above 3")
         self.queue.append(req)
 
+    def _half_of(self, src: torch.Tensor) -> torch.Tensor:
+        """The FP16 copy of a source tensor (converted on the server's stream once, shared)."""
+        key = src.data_ptr()
+        ent = self._half.get(key)
+        if ent is None:
+            ent = [src, fast.to_fp16(src, stream=self.stream), 0]
+            self._half[key] = ent
+        ent[2] += 1
+        return ent[1]
+
+    def _release_half(self, job):
+        if self.precision != L.PREC_FP16:
+            return
+        for s in job.srcs:
+            ent = self._half.get(s.data_ptr())
+            if ent is not None:
+                ent[2] -= 1
+                if ent[2] == 0:
+                    del self._half[s.data_ptr()]
+
     def _admit(self, now: float):
         needs = [footprint(q, self.shared_sources) for q in self.queue]
         n, reject = admissions(needs, len(self.free_slots), self.used, self.budget)
@@ -188,7 +226,7 @@ class DepthServer:
             req = self.queue.pop(0)
             need = footprint(req, self.shared_sources)
             slot = self.free_slots.pop()
-            job = _Job(req, slot, self.dev, self.stream, self.plane_chunk)
+            job = _Job(req, slot, self.dev, self.stream, self.plane_chunk, self.precision, self._half_of)
             L.check(L.load().mvs_server_set_job(self._h, slot, ctypes.addressof(job.args),
                                                 job.rec.data_ptr(), self.plane_chunk), "server_set_job")
             job.admitted = now
@@ -234,11 +272,19 @@ class DepthServer:
                         self._start_pm(j)
         for j in [j for j in self.active.values() if j.phase == "pm" and j.pm_started]:
             j.pm.it0 = j.pm_done
-            L.check(lib.mvs_pm_refine(ctypes.addressof(j.pm), sh), "pm_refine")
-            self.launch_count += 2
+            L.check(lib.mvs_pm_refine(ctypes.addressof(j.pm), j.pm_stream.cuda_stream), "pm_refine")
+            self.launch_count += 1 + 10
             j.pm_done += 1
             if j.pm_done == j.req.pm_iters:
-                j.phase = "done"
+                # results queued on the job's stream; collected once its event has completed
+                with torch.cuda.stream(j.pm_stream):
+                    j.h_depth = torch.empty((j.H, j.W), dtype=torch.float32).pin_memory()
+                    j.h_depth.copy_(j.pm_depth, non_blocking=True)
+                    j.h_score = j.pm_score.to("cpu", non_blocking=True)
+                    j.h_normal = j.pm_normal.to("cpu", non_blocking=True)
+                    j.pm_done_event = torch.cuda.Event()
+                    j.pm_done_event.record(j.pm_stream)
+                j.phase = "pm_copy"
         for j in self.active.values():
             if j.phase == "pm" and not j.pm_started:
                 j.pm_started = True          # PatchMatch starts on the step after the sweep ends
@@ -246,25 +292,31 @@ class DepthServer:
         for j in done:
             j.h_depth = torch.empty((j.H, j.W), dtype=torch.float32).pin_memory()
             with torch.cuda.stream(self.stream):
-                j.h_depth.copy_(j.depth if not j.req.pm_iters else j.pm_depth, non_blocking=True)
-                if j.req.pm_iters:
-                    j.h_score = j.pm_score.to("cpu", non_blocking=True)
-                    j.h_normal = j.pm_normal.to("cpu", non_blocking=True)
+                j.h_depth.copy_(j.depth, non_blocking=True)
         self.stream.synchronize()
+        done += [j for j in self.active.values() if j.phase == "pm_copy" and j.pm_done_event.query()]
         t = time.perf_counter()
         for j in done:
             self.results.append(Result(j.req.rid, j.h_depth.numpy(), getattr(j, "h_score", None),
                                        getattr(j, "h_normal", None), j.req.arrival, j.admitted, t))
+            self._release_half(j)
             del self.active[j.slot]
             self.free_slots.append(j.slot)
             self.used -= j.bytes
+        if not done and self.active and all(j.phase == "pm_copy" for j in self.active.values()):
+            time.sleep(2e-4)                 # only PatchMatch copies in flight: do not spin hot
         self.steps += 1
         return len(done)
 
     def _start_pm(self, j: _Job):
         req = j.req
         H, W = j.H, j.W
-        with torch.cuda.stream(self.stream):
+        j.pm_stream = self.pm_streams[self._pm_next % len(self.pm_streams)]
+        self._pm_next += 1
+        ready = torch.cuda.Event()
+        ready.record(self.stream)              # after the job's finalize
+        j.pm_stream.wait_event(ready)
+        with torch.cuda.stream(j.pm_stream):
             j.pm_ray = fast.rays_world((H, W), req.ref_cam)
             j.pm_depth = j.depth.clone()
             rng = np.random.default_rng(req.seed)
@@ -323,9 +375,10 @@ def serve(requests, server: DepthServer, realtime: bool = True):
     return sorted(server.results, key=lambda r: r.rid), time.perf_counter() - t0
 
 
-def serve_plain(requests, realtime: bool = True):
+def serve_plain(requests, realtime: bool = True, precision: str = "fp32"):
     """The plain per-request comparator: FIFO, one request at a time, mvs_sweep + finalize
-    (+ PatchMatch), results copied back. Same arrival trace semantics as serve()."""
+    (+ PatchMatch), results copied back. Same arrival trace semantics as serve(). precision
+    "fp16": the sweep reads FP16 copies of the sources, as the FP16 server does."""
     from .dense import sweep, finalize
     dev = L.require_cuda()
     pending = sorted(requests, key=lambda q: q.arrival)
@@ -341,8 +394,10 @@ def serve_plain(requests, realtime: bool = True):
                 for s in req.srcs]
         mu, sd = fast.ref_stats(ref, req.r)
         hyp = Hypotheses.planes_inv(req.planes_inv)
-        st = sweep(ref, mu, sd, None, srcs, _geo(req.ref_cam, req.src_cams), hyp, req.r, req.top_k,
-                   ref_cam=fast.cam_row(req.ref_cam))
+        half = precision == "fp16"
+        st = sweep(ref, mu, sd, None, [fast.to_fp16(s) for s in srcs] if half else srcs,
+                   _geo(req.ref_cam, req.src_cams), hyp, req.r, req.top_k, ref_cam=fast.cam_row(req.ref_cam),
+                   precision=L.PREC_FP16 if half else L.PREC_FP32)
         depth = finalize(hyp, st)
         score = normal = None
         if req.pm_iters:

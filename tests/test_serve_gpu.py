@@ -56,3 +56,17 @@ def test_budget_forces_queueing_without_changing_results():
     too_big.submit(_requests()[0])
     with pytest.raises(MemoryError):
         too_big.step(0.0)
+
+
+def test_fp16_server_matches_the_plain_fp16_path_with_patchmatch_overlapped():
+    """The FP16-storage server (sources converted once and shared, FP32 sums) against the plain
+    per-request path with the same FP16 sources: the same bits per job, PatchMatch jobs included
+    (they run on the server's PatchMatch streams, overlapping the sweep steps)."""
+    from py_ortho_b200.serve import DepthServer, serve, serve_plain
+    srv = DepthServer(plane_chunk=8, max_slots=8, precision="fp16", pm_streams=2)
+    mix, _ = serve(_requests(), srv, realtime=False)
+    plain, _ = serve_plain(_requests(), realtime=False, precision="fp16")
+    assert [r.rid for r in mix] == list(range(6))
+    for a, b in zip(mix, plain):
+        _check(a, b)
+    assert not srv._half                         # every FP16 copy released with its last job
