@@ -71,10 +71,18 @@ typedef enum mvs_precision {
     MVS_PREC_FP32 = 0,      /* plain: float32 images and tiles, FP32 window sums                   */
     MVS_PREC_FP16 = 1,      /* FP16 images (src pointers are __half), FP32 window sums; PLANES only;
                                FP64 homography and parabola                                        */
-    MVS_PREC_FP64_SUMS = 2  /* float32 images and tiles, window sums in float64 as the reference
+    MVS_PREC_FP64_SUMS = 2, /* float32 images and tiles, window sums in float64 as the reference
                                keeps them (_sweep.h:85-178): its NCC to ~1 float32 ulp even on
                                bright low-texture windows, where FP32 sums differ by up to ~1e-3;
                                single-view calls (mvs_sweep*) only, slower stages B and C        */
+    MVS_PREC_FP32_COMP = 3, /* compensated FP32 window sums: reference and warped values shifted by
+                               one pivot per tile (the tile's mean reference value), vertical sums
+                               of the variance / covariance terms with Kahan compensation, and the
+                               reference window statistics formed from the pivoted tile (the `mu`
+                               and `sd` arguments are not read). Closer to an all-float64 sweep than
+                               the reference's own float32 statistics; PLANES, top_k <= 2,
+                               single-view calls only                                              */
+    MVS_PREC_FP16_COMP = 4  /* MVS_PREC_FP32_COMP with FP16 source storage (src are __half)        */
 } mvs_precision;
 
 typedef struct mvs_sweep_args {

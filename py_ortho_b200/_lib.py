@@ -24,7 +24,7 @@ BAND_MIN_POINTS = 50
 
 OK, ERR_VALUE, ERR_MEMORY, ERR_CUDA, ERR_TIMEOUT, ERR_UNSUPPORTED = range(6)
 HYP_MAPS, HYP_LINEAR, HYP_REFINE, HYP_PLANES = range(4)
-PREC_FP32, PREC_FP16, PREC_FP64_SUMS = 0, 1, 2
+PREC_FP32, PREC_FP16, PREC_FP64_SUMS, PREC_FP32_COMP, PREC_FP16_COMP = 0, 1, 2, 3, 4
 
 vp = C.c_void_p
 i32 = C.c_int32

@@ -200,7 +200,10 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
         mvs_status st = validate_sweep(a);
         if (st != MVS_OK) { batch_free(b); return st; }
         if (a->hyp.kind != MVS_HYP_PLANES) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d must use MVS_HYP_PLANES", j); }
-        if (a->precision == MVS_PREC_FP64_SUMS) { batch_free(b); return fail(MVS_ERR_UNSUPPORTED, "batch: float64 window sums run on the single-view kernel (mvs_sweep) only"); }
+        if (a->precision == MVS_PREC_FP64_SUMS || a->precision == MVS_PREC_FP32_COMP || a->precision == MVS_PREC_FP16_COMP) {
+            batch_free(b);
+            return fail(MVS_ERR_UNSUPPORTED, "batch: float64 and compensated window sums run on the single-view kernel (mvs_sweep) only");
+        }
         if ((a->precision == MVS_PREC_FP16) != b->f16) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: all jobs need the same precision"); }
         if (a->i1 - a->i0 > MVS_MAX_PLANES_PER_CALL) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d has more than %d planes", j, MVS_MAX_PLANES_PER_CALL); }
         if (a->H == 0 || a->W == 0 || a->i1 == a->i0) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d is empty", j); }
@@ -398,7 +401,8 @@ extern "C" mvs_status mvs_server_create(int32_t max_slots, int32_t max_items, in
     *out = nullptr;
     if (max_slots < 1 || max_items < 1) return fail(MVS_ERR_VALUE, "server: needs slots and items");
     if (max_radius < 0 || max_radius > MVS_MAX_RADIUS) return fail(MVS_ERR_VALUE, "server: radius outside 0..%d", MVS_MAX_RADIUS);
-    if (precision == MVS_PREC_FP64_SUMS) return fail(MVS_ERR_UNSUPPORTED, "server: float64 window sums run on the single-view kernel (mvs_sweep) only");
+    if (precision == MVS_PREC_FP64_SUMS || precision == MVS_PREC_FP32_COMP || precision == MVS_PREC_FP16_COMP)
+        return fail(MVS_ERR_UNSUPPORTED, "server: float64 and compensated window sums run on the single-view kernel (mvs_sweep) only");
     if (precision != MVS_PREC_FP32 && precision != MVS_PREC_FP16) return fail(MVS_ERR_VALUE, "server: unknown precision");
     mvs_server* s = new mvs_server();
     s->max_slots = max_slots;
@@ -431,7 +435,8 @@ extern "C" mvs_status mvs_server_set_job(mvs_server* s, int32_t slot, const mvs_
     if (slot < 0 || slot >= s->max_slots) return fail(MVS_ERR_VALUE, "server: slot %d outside 0..%d", slot, s->max_slots - 1);
     MVS_TRY(validate_sweep(job));
     if (job->hyp.kind != MVS_HYP_PLANES) return fail(MVS_ERR_VALUE, "server: jobs must use MVS_HYP_PLANES");
-    if (job->precision == MVS_PREC_FP64_SUMS) return fail(MVS_ERR_UNSUPPORTED, "server: float64 window sums run on the single-view kernel (mvs_sweep) only");
+    if (job->precision == MVS_PREC_FP64_SUMS || job->precision == MVS_PREC_FP32_COMP || job->precision == MVS_PREC_FP16_COMP)
+        return fail(MVS_ERR_UNSUPPORTED, "server: float64 and compensated window sums run on the single-view kernel (mvs_sweep) only");
     if ((job->precision == MVS_PREC_FP16) != s->f16) return fail(MVS_ERR_VALUE, "server: job precision differs from the server's");
     if (job->r > (s->rmax <= 3 ? 3 : 7)) return fail(MVS_ERR_VALUE, "server: job radius above the server's");
     if (job->i1 - job->i0 > MVS_MAX_PLANES_PER_CALL || job->i1 <= job->i0) return fail(MVS_ERR_VALUE, "server: bad plane range");

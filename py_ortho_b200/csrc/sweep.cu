@@ -42,12 +42,12 @@ static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r) 
     return e == CUDA_SUCCESS;
 }
 
-template <int R, int KMAX, bool PLANES, bool F16, bool X64>
+template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP>
 __global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ SweepParams p) {
     extern __shared__ __align__(128) float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, KMAX, PLANES, F16, true, true, X64>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
+    sweep_tile<R, KMAX, PLANES, F16, true, true, X64, CMP>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
                                                  p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
 }
 
@@ -95,10 +95,10 @@ __global__ void finalize_kernel(int H, int W, int kind, int n, int t0, const flo
 
 // ------------------------------------------------------------------------------ launcher
 
-template <int R, int KMAX, bool PLANES, bool F16, bool X64>
+template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP>
 static mvs_status launch_sweep(const SweepParams& p, dim3 grid, cudaStream_t st) {
-    auto kern = sweep_kernel<R, KMAX, PLANES, F16, X64>;
-    const size_t smem = Geom<R>::smem_bytes();
+    auto kern = sweep_kernel<R, KMAX, PLANES, F16, X64, CMP>;
+    const size_t smem = Geom<R>::smem_bytes() + (CMP ? Geom<R>::count_bytes() : 0);
     // the attribute is per function and per device: set it for the current device every time
     MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "sweep: shared memory attribute");
@@ -106,24 +106,30 @@ static mvs_status launch_sweep(const SweepParams& p, dim3 grid, cudaStream_t st)
     return check_launch("sweep kernel");
 }
 
-template <int KMAX, bool PLANES, bool F16, bool X64 = false>
+template <int KMAX, bool PLANES, bool F16, bool X64 = false, bool CMP = false>
 static mvs_status dispatch_r(int r, const SweepParams& p, dim3 grid, cudaStream_t st) {
     switch (r) {
-        case 0: return launch_sweep<0, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 1: return launch_sweep<1, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 2: return launch_sweep<2, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 3: return launch_sweep<3, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 4: return launch_sweep<4, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 5: return launch_sweep<5, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 6: return launch_sweep<6, KMAX, PLANES, F16, X64>(p, grid, st);
-        case 7: return launch_sweep<7, KMAX, PLANES, F16, X64>(p, grid, st);
+        case 0: return launch_sweep<0, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 1: return launch_sweep<1, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 2: return launch_sweep<2, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 3: return launch_sweep<3, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 4: return launch_sweep<4, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 5: return launch_sweep<5, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 6: return launch_sweep<6, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 7: return launch_sweep<7, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
     }
     return fail(MVS_ERR_VALUE, "sweep: window radius %d outside 0..%d", r, MVS_MAX_RADIUS);
 }
 
-static mvs_status dispatch(int r, int kmax, bool planes, bool f16, bool x64, const SweepParams& p, dim3 grid,
+static mvs_status dispatch(int r, int kmax, bool planes, int precision, const SweepParams& p, dim3 grid,
                            cudaStream_t st) {
-    if (x64) {
+    const bool f16 = precision == MVS_PREC_FP16 || precision == MVS_PREC_FP16_COMP;
+    if (precision == MVS_PREC_FP32_COMP || precision == MVS_PREC_FP16_COMP) {
+        if (!planes || kmax > 2) return fail(MVS_ERR_UNSUPPORTED, "sweep: compensated sums need MVS_HYP_PLANES and top_k <= 2");
+        return f16 ? dispatch_r<2, true, true, false, true>(r, p, grid, st)
+                   : dispatch_r<2, true, false, false, true>(r, p, grid, st);
+    }
+    if (precision == MVS_PREC_FP64_SUMS) {
         if (planes) return kmax <= 2 ? dispatch_r<2, true, false, true>(r, p, grid, st)
                                      : dispatch_r<8, true, false, true>(r, p, grid, st);
         return kmax <= 2 ? dispatch_r<2, false, false, true>(r, p, grid, st) : dispatch_r<8, false, false, true>(r, p, grid, st);
@@ -151,7 +157,7 @@ mvs_status validate_sweep(const mvs_sweep_args* a) {
     if (a->top_k < 1) return fail(MVS_ERR_VALUE, "sweep: top_k must be >= 1");
     if (!a->geo) return fail(MVS_ERR_VALUE, "geo must be (n_sources, 18)");
     if (a->i1 < a->i0) return fail(MVS_ERR_VALUE, "sweep: empty or reversed hypothesis range");
-    if (a->precision != MVS_PREC_FP32 && a->precision != MVS_PREC_FP16 && a->precision != MVS_PREC_FP64_SUMS)
+    if (a->precision < MVS_PREC_FP32 || a->precision > MVS_PREC_FP16_COMP)
         return fail(MVS_ERR_VALUE, "sweep: unknown precision");
     const int kind = a->hyp.kind;
     if (kind < MVS_HYP_MAPS || kind > MVS_HYP_PLANES) return fail(MVS_ERR_VALUE, "sweep: unknown hypothesis kind");
@@ -179,8 +185,11 @@ mvs_status validate_sweep(const mvs_sweep_args* a) {
         if ((kind == MVS_HYP_LINEAR || kind == MVS_HYP_REFINE) && (!a->hyp.base || !a->hyp.step))
             return fail(MVS_ERR_VALUE, "sweep: null hypothesis base/step");
     }
-    if (a->precision == MVS_PREC_FP16 && kind != MVS_HYP_PLANES)
+    if ((a->precision == MVS_PREC_FP16 || a->precision == MVS_PREC_FP16_COMP) && kind != MVS_HYP_PLANES)
         return fail(MVS_ERR_UNSUPPORTED, "sweep: FP16 storage needs MVS_HYP_PLANES");
+    if ((a->precision == MVS_PREC_FP32_COMP || a->precision == MVS_PREC_FP16_COMP) &&
+        (kind != MVS_HYP_PLANES || (a->top_k < a->n_src ? a->top_k : a->n_src) > 2))
+        return fail(MVS_ERR_UNSUPPORTED, "sweep: compensated sums need MVS_HYP_PLANES and top_k <= 2");
     return MVS_OK;
 }
 
@@ -273,8 +282,7 @@ mvs_status sweep_range(const mvs_sweep_args* a, int i0, int i1, float* rec_ws, i
     p.nchunks = used;
     p.r = a->r;
     dim3 grid((a->W + TW - 1) / TW, (a->H + TH - 1) / TH, used);
-    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision == MVS_PREC_FP16,
-                     a->precision == MVS_PREC_FP64_SUMS, p, grid, st));
+    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision, p, grid, st));
     if (used > 1) {
         const long long HW = (long long)a->H * a->W;
         merge_kernel<<<(unsigned)((HW + 255) / 256), 256, 0, st>>>(HW, used, i0, i1, p.ppc, rec_ws, a->best, a->prev,

@@ -96,6 +96,9 @@ struct Geom {
     static constexpr int P = 16;                   // stage-B outputs per thread (one row segment)
     static constexpr int NSEG = TW / P;
     static constexpr int NIN = P + 2 * RA;         // stage-B inputs per segment
+    static constexpr size_t count_bytes() {      // compensated mode: uint8 horizontal window counts
+        return ((size_t)HR * TW + 15) & ~(size_t)15;
+    }
     static constexpr size_t smem_bytes() {       // sJ, sI, sH, winner state (6 planes), sC
         return (size_t)HR * JP * 4 * 2 + (size_t)HR * TW * 16 + (size_t)6 * TH * TW * 4 +
                sizeof(Coef) * MVS_MAX_SOURCES;
@@ -522,6 +525,159 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
     }
 }
 
+// ---- compensated window sums (MVS_PREC_FP32_COMP / MVS_PREC_FP16_COMP)
+//
+// A bright, low-texture window (grey ~1.5, deviations ~0.05) makes the plain form's moments
+// m2 - mj^2 and mij - mu mj differences of numbers ~2.25 that agree to ~3 digits, so float32
+// rounding of the sums (and of the reference statistics) reaches the NCC a thousand-fold. This form
+// removes the large common part before anything is summed: the tile's reference values and every
+// warped source value are shifted by one pivot per tile (the mean reference value of the tile's
+// pixels), the window sums of the shifted values are accumulated with Kahan compensation in the
+// vertical direction (the variance and covariance terms), and the reference window statistics are
+// formed from the shifted tile (zero padding outside the image, divided by k^2, floor 1e-6 on the
+// variance: the reference's definitions). With I' = I - p and J' = J - p:
+//   var(J) = E[J'^2] - E[J']^2,   E[IJ] - mu E[J] = E[I'J'] - mu' E[J'] + p (E[I'] - mu'),
+// mu' = mu - p; E[] over the window's valid samples. When every sample of the tile is valid the
+// windows are full and E[I'] = mu' exactly, so the last term is zero and is not formed; otherwise
+// the masked sum of I' is accumulated as a fifth quantity (the counts then move to a byte array).
+
+template <int R, bool WITHV>
+__device__ __forceinline__ void stage_b_cmp(const float* sJ, const float* sI, float4* sH, unsigned char* sV, int tid) {
+    using G = Geom<R>;
+    constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
+    if (tid >= HR * NSEG) return;
+    const int sg = tid / HR, hy = tid - sg * HR;
+    const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
+    const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
+    float v[NIN], s0[NIN], s1[NIN], s2[NIN], s3[NIN];
+#pragma unroll
+    for (int q = 0; q < NIN / 4; ++q) {
+        const float4 a = jr[q], b = ir[q];
+        const float jv[4] = {a.x, a.y, a.z, a.w}, iv[4] = {b.x, b.y, b.z, b.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int t = 4 * q + u;
+            float jz = jv[u];
+            if constexpr (WITHV) {
+                const bool ok = jz == jz;
+                jz = ok ? jz : 0.f;
+                v[t] = ok ? 1.f : 0.f;
+                s0[t] = ok ? iv[u] : 0.f;
+            }
+            s1[t] = jz;
+            s2[t] = __fmul_rn(jz, jz);
+            s3[t] = __fmul_rn(jz, iv[u]);
+        }
+    }
+    float a0 = 0.f, a4 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;
+#pragma unroll
+    for (int t = RA - R; t <= RA + R; ++t) {
+        if constexpr (WITHV) {
+            a0 = __fadd_rn(a0, v[t]);
+            a4 = __fadd_rn(a4, s0[t]);
+        }
+        a1 = __fadd_rn(a1, s1[t]);
+        a2 = __fadd_rn(a2, s2[t]);
+        a3 = __fadd_rn(a3, s3[t]);
+    }
+    float4* row = sH + hy * TW + P * sg;
+    unsigned char* crow = sV + hy * TW + P * sg;
+    const int kx = (sg + hy) & 7;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+        if (j > 0) {
+            const int tn = RA + R + j, to = RA - R + j - 1;
+            if constexpr (WITHV) {
+                a0 = __fadd_rn(a0, __fsub_rn(v[tn], v[to]));
+                a4 = __fadd_rn(a4, __fsub_rn(s0[tn], s0[to]));
+            }
+            a1 = __fadd_rn(a1, __fsub_rn(s1[tn], s1[to]));
+            a2 = __fadd_rn(a2, __fsub_rn(s2[tn], s2[to]));
+            a3 = __fadd_rn(a3, __fsub_rn(s3[tn], s3[to]));
+        }
+        row[j ^ kx] = make_float4(a4, a1, a2, a3);
+        if constexpr (WITHV) crow[j] = (unsigned char)a0;
+    }
+}
+
+// Kahan step: s += x with the running compensation c (s - c is the better estimate).
+__device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
+    const float y = __fsub_rn(x, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+}
+
+// `mu` holds the pivoted window mean mu' = mu - p and `rsd` the reciprocal window deviation, both
+// formed from the pivoted reference tile.
+template <int R, int KMAX, bool WITHV>
+__device__ __forceinline__ void stage_c_cmp(const float4* sH, const unsigned char* sV, int c, int y0, const float* mu,
+                                            const float* rsd, float pv, float (&topk)[ROWS][KMAX], float* total,
+                                            bool bottom, int nlist) {
+    constexpr int K = 2 * R + 1;
+    const float k2 = (float)(K * K), inv_k2 = 1.0f / (float)(K * K);
+    static_assert(ROWS % 8 == 0, "stage C rows must start on a multiple of 8");
+    int sw[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
+    const float4* col = sH + y0 * TW;
+    const unsigned char* ccol = sV + y0 * TW + c;
+    float cv = 0.f, ci = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
+    float ej = 0.f, ejj = 0.f, eji = 0.f;            // Kahan compensations
+#pragma unroll
+    for (int t = 0; t < K; ++t) {
+        const float4 h = col[t * TW + sw[t & 7]];
+        if constexpr (WITHV) {
+            cv = __fadd_rn(cv, (float)ccol[t * TW]);
+            ci = __fadd_rn(ci, h.x);
+        }
+        kahan_add(cj, ej, h.y);
+        kahan_add(cjj, ejj, h.z);
+        kahan_add(cji, eji, h.w);
+    }
+#pragma unroll
+    for (int j = 0; j < ROWS; ++j) {
+        if (j > 0) {
+            const float4 hn = col[(j + 2 * R) * TW + sw[(j + 2 * R) & 7]];
+            const float4 ho = col[(j - 1) * TW + sw[(j - 1) & 7]];
+            if constexpr (WITHV) {
+                cv = __fadd_rn(cv, __fsub_rn((float)ccol[(j + 2 * R) * TW], (float)ccol[(j - 1) * TW]));
+                ci = __fadd_rn(ci, __fsub_rn(hn.x, ho.x));
+            }
+            kahan_add(cj, ej, hn.y);
+            kahan_add(cj, ej, -ho.y);
+            kahan_add(cjj, ejj, hn.z);
+            kahan_add(cjj, ejj, -ho.z);
+            kahan_add(cji, eji, hn.w);
+            kahan_add(cji, eji, -ho.w);
+        }
+        float ncc;
+        if (WITHV && cv * 10.f <= 9.f * k2) {
+            ncc = -1.f;
+        } else {
+            const float rc = (!WITHV || cv == k2) ? inv_k2 : __frcp_rn(cv);
+            const float mj = __fmul_rn(__fsub_rn(cj, ej), rc), m2 = __fmul_rn(__fsub_rn(cjj, ejj), rc);
+            const float mij = __fmul_rn(__fsub_rn(cji, eji), rc);
+            const float var = __fsub_rn(m2, __fmul_rn(mj, mj));
+            const float rsdj = var > 1e-6f ? rsqrtf(var) : 1000.f;
+            float cov = __fsub_rn(mij, __fmul_rn(mu[j], mj));
+            if (WITHV) cov = __fadd_rn(cov, __fmul_rn(pv, __fsub_rn(__fmul_rn(ci, rc), mu[j])));
+            ncc = __fmul_rn(cov, __fmul_rn(rsd[j], rsdj));
+            ncc = ncc > 1.f ? 1.f : (ncc < -1.f ? -1.f : ncc);
+        }
+        if (bottom) total[j] = __fadd_rn(total[j], ncc);
+        float x = ncc;
+#pragma unroll
+        for (int q = 0; q < KMAX; ++q) {
+            if (q < nlist) {
+                const float hi = fmaxf(topk[j][q], x), lo = fminf(topk[j][q], x);
+                topk[j][q] = bottom ? lo : hi;
+                x = bottom ? hi : lo;
+            }
+        }
+    }
+}
+
 // ---- the reference tile by TMA (single-view kernel): one 2D tiled bulk copy per CTA, completed
 // on an mbarrier. The copy's box is the tile with its halo, JP x HR floats starting at
 // (tx - RA, ty - R): x is a multiple of 4 floats (16 bytes), rows outside the image read as 0,
@@ -579,7 +735,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // flight; more registers - the single-view kernel, whose radius is a template argument, uses it).
 // REF_TMA: the reference tile arrives by TMA when p.ref_tma is set (the single-view kernel, whose
 // parameters hold the tensor map; `smem` must then be 128-byte aligned).
-template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false, bool X64 = false>
+template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false, bool X64 = false,
+          bool CMP = false>
 __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
     using G = Geom<R>;
     constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
@@ -629,9 +786,10 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
         const int ly = seg * ROWS + j, gy = ty + ly;
         const bool in = gx < W && gy < H;
         const long long o = (long long)gy * W + gx;
-        mu[j] = in ? __ldg(p.mu + o) : 0.f;
+        // (compensated mode: formed from the pivoted tile below instead)
+        mu[j] = in && !CMP ? __ldg(p.mu + o) : 0.f;
         // X64: the deviation itself (stage C divides in float64); else its reciprocal
-        rsd[j] = in ? (X64 ? __ldg(p.sd + o) : 1.0f / __ldg(p.sd + o)) : 0.f;
+        rsd[j] = in && !CMP ? (X64 ? __ldg(p.sd + o) : 1.0f / __ldg(p.sd + o)) : 0.f;
         const bool load = in && !to_rec && !p.fresh;
         const int w = ly * TW + c;
         sW[w] = load ? p.best[o] : -2.f;
@@ -665,6 +823,64 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
         }
     }
 #endif
+    // compensated mode: pivot the reference tile and form its window statistics from it
+    float pv = 0.f;
+    unsigned char* sV = reinterpret_cast<unsigned char*>(sC + MVS_MAX_SOURCES);   // byte counts
+    if constexpr (CMP) {
+        __shared__ float red[2 * (NT / 32)];
+        __syncthreads();                       // the reference tile is complete (thread loads or TMA)
+        float su = 0.f, nn = 0.f;
+#pragma unroll
+        for (int j = 0; j < ROWS; ++j) {
+            const int ly = seg * ROWS + j;
+            if (gx < W && ty + ly < H) {
+                su = __fadd_rn(su, sI[(ly + R) * JP + RA + c]);
+                nn += 1.f;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            su = __fadd_rn(su, __shfl_xor_sync(0xffffffffu, su, o));
+            nn += __shfl_xor_sync(0xffffffffu, nn, o);
+        }
+        if ((tid & 31) == 0) {
+            red[tid >> 5] = su;
+            red[NT / 32 + (tid >> 5)] = nn;
+        }
+        __syncthreads();
+        su = 0.f;
+        nn = 0.f;
+        for (int w = 0; w < NT / 32; ++w) {   // every thread sums the warp totals in the same order
+            su = __fadd_rn(su, red[w]);
+            nn += red[NT / 32 + w];
+        }
+        pv = nn > 0.f ? __fdiv_rn(su, nn) : 0.f;
+        for (int e = tid; e < HR * JP; e += NT) sI[e] = __fsub_rn(sI[e], pv);
+        __syncthreads();
+        // mu' = sum(I') / k^2 over the zero-padded window (I' = -p outside the image), var =
+        // sum(I'^2) / k^2 - mu'^2, sd = sqrt(max(var, 1e-6)): the reference's statistics, pivoted
+        const float inv_k2 = 1.0f / (float)(K * K);
+#pragma unroll
+        for (int j = 0; j < ROWS; ++j) {
+            const int ly = seg * ROWS + j;
+            float s1 = 0.f, s2 = 0.f;
+#pragma unroll 1
+            for (int dy = 0; dy < K; ++dy) {
+                const float* rowp = sI + (ly + dy) * JP + (RA - R) + c;
+#pragma unroll
+                for (int dx = 0; dx < K; ++dx) {
+                    const float v = rowp[dx];
+                    s1 = __fadd_rn(s1, v);
+                    s2 = __fmaf_rn(v, v, s2);
+                }
+            }
+            const float m = __fmul_rn(s1, inv_k2);
+            const float var = __fsub_rn(__fmul_rn(s2, inv_k2), __fmul_rn(m, m));
+            const bool in = gx < W && ty + ly < H;
+            mu[j] = in ? m : 0.f;
+            rsd[j] = in ? __frcp_rn(__fsqrt_rn(var > 1e-6f ? var : 1e-6f)) : 0.f;
+        }
+    }
 
     for (int i = pa; i < pb; ++i) {
         float topk[ROWS][KMAX];
@@ -715,7 +931,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                     for (int k = 0; k < MR; ++k) {
                         if ((k + 1) * SEG <= HR || seg + k * SEG < HR) {
                             any_invalid |= Jv[k] != Jv[k];
-                            col[k * SEG * JP] = Jv[k];
+                            col[k * SEG * JP] = CMP ? __fsub_rn(Jv[k], pv) : Jv[k];
                         }
                     }
 #pragma unroll
@@ -724,7 +940,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                         if (e0 < XS) {
                             const int hy = e0 / XW, hc = TW + (e0 - hy * XW);
                             any_invalid |= Jv[MR + m] != Jv[MR + m];
-                            sJ[hy * JP + (RA - R) + hc] = Jv[MR + m];
+                            sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(Jv[MR + m], pv) : Jv[MR + m];
                         }
                     }
                 } else if (cf.inside && tile_inside) {
@@ -735,7 +951,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                             const int hy = e / HC, hc = e - hy * HC;
                             const float J = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
                             any_invalid |= J != J;
-                            sJ[hy * JP + (RA - R) + hc] = J;
+                            sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(J, pv) : J;
                         }
                     }
                 } else {
@@ -748,7 +964,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                             const bool in = gy >= 0 && gy < H && gxx >= 0 && gxx < W;
                             const float J = sample_plane<F16>(cf, img, sw, sh, (float)hc, (float)hy, in);
                             any_invalid |= J != J;
-                            sJ[hy * JP + (RA - R) + hc] = J;
+                            sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(J, pv) : J;
                         }
                     }
                 }
@@ -759,7 +975,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                     const int gy = ty - R + hy, gxx = tx - R + hc;
                     float J = qnan();
                     if (gy >= 0 && gy < H && gxx >= 0 && gxx < W) J = sample_ray(p, p.src[s], i, gxx, gy);
-                    sJ[hy * JP + (RA - R) + hc] = J;
+                    sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(J, pv) : J;
                 }
             }
             // every sample of this (hypothesis, source) valid -> the count is k^2 everywhere and
@@ -767,7 +983,13 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             const bool all_valid = !__syncthreads_or(any_invalid);
             // ---- B: horizontal window sums of (V, J, J^2, J I), one 16-column row segment per
             // thread: products once per input, running sums along the segment
-            if constexpr (X64) {
+            if constexpr (CMP) {
+                if (all_valid) {
+                    stage_b_cmp<R, false>(sJ, sI, sH, sV, tid);
+                } else {
+                    stage_b_cmp<R, true>(sJ, sI, sH, sV, tid);
+                }
+            } else if constexpr (X64) {
                 if (all_valid) {
                     stage_b64<R, false>(sJ, sI, sH, tid);
                 } else {
@@ -780,7 +1002,13 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             }
             __syncthreads();
             // ---- C: vertical running sums down the column, NCC, top-k insertion
-            if constexpr (X64) {
+            if constexpr (CMP) {
+                if (all_valid) {
+                    stage_c_cmp<R, KMAX, false>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
+                } else {
+                    stage_c_cmp<R, KMAX, true>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
+                }
+            } else if constexpr (X64) {
                 if (all_valid) {
                     stage_c64<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
                 } else {

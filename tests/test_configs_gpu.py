@@ -115,3 +115,56 @@ def test_c2_bench_step_row_bands_parity():
         reps.append(rep)
         assert rep["decided"] > 0.5 * (y1 - y0) * W
     print("C2 band parity:", reps)
+
+
+def test_c3_precision_variant_on_ten_scenes():
+    """C3: C1's shape (640 x 480, 4 sources, 128 planes over [35, 55] m, 5 x 5, best 2) on ten seeded
+    scenes; depth error of each storage / summation form against the all-float64 oracle sweep of
+    the same planes (float64 statistics, sums, NCC and parabola): median and 99th percentile over
+    all pixels. Forms: plain FP32, FP16 storage, and the compensated sums (pivoted tile, Kahan
+    vertical sums, statistics from the pivoted tile) with FP16 and FP32 storage. Bar: median
+    <= 0.1 % for every form."""
+    from py_ortho_b200 import _lib as L
+    from py_ortho_b200 import dense, fast, scene as S
+    forms = {"fp32": L.PREC_FP32, "fp16": L.PREC_FP16, "fp16_comp": L.PREC_FP16_COMP, "fp32_comp": L.PREC_FP32_COMP}
+    planes = S.plane_list(35.0, 55.0, 128)
+    r, top_k = 2, 2
+    hyp = dense.Hypotheses.planes_inv(planes)
+    errs = {k: [] for k in forms}
+    scenes = []
+    for seed in range(10):
+        sc = S.make_scene("c1", seed=100 + seed, device="cuda")
+        ref = sc.grey(sc.ref)
+        srcs = [sc.grey(s) for s in sc.srcs]
+        geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+        H, W = ref.shape
+        ref_d = _dev(ref)
+        mu, sd = fast.ref_stats(ref_d, r)
+        s32 = [_dev(s) for s in srcs]
+        s16 = [fast.to_fp16(s) for s in s32]
+        outs = {}
+        for name, prec in forms.items():
+            st = dense.sweep(ref_d, mu, sd, None, s16 if prec in (L.PREC_FP16, L.PREC_FP16_COMP) else s32, geo, hyp, r,
+                             top_k, ref_cam=sc.ref_cam.row(), precision=prec)
+            outs[name] = dense.finalize(hyp, st).cpu().numpy().astype(np.float64)
+        scenes.append((ref, srcs, O.rays_world((H, W), sc.ref_cam), geo, outs))
+
+    def oracle64(item):
+        ref, srcs, ray, geo, _ = item
+        H, W = ref.shape
+        d64, _, _ = O.sweep_fp64(ref, srcs, ray, geo, [np.full((H, W), p, np.float64) for p in planes], r, top_k)
+        return d64
+
+    with ThreadPoolExecutor(5) as ex:
+        d64s = list(ex.map(oracle64, scenes))
+    for (_, _, _, _, outs), d64 in zip(scenes, d64s):
+        for name in forms:
+            errs[name].append(np.abs(outs[name] - d64) / d64)
+    report = {}
+    for name in forms:
+        e = np.concatenate([x.ravel() for x in errs[name]])
+        report[name] = {"median": float(np.median(e)), "p99": float(np.percentile(e, 99)),
+                        "p999": float(np.percentile(e, 99.9)), "max": float(e.max())}
+    print("C3 depth error vs the float64 oracle (10 scenes, 640x480, 128 planes):", report)
+    for name in forms:
+        assert report[name]["median"] <= 1e-3, (name, report[name])
