@@ -95,13 +95,15 @@ def test_validation_errors_need_no_device():
     p.S = 17
     assert lib.mvs_pm_refine(ctypes.addressof(p), None) == L.OK
     assert lib.mvs_batch_create(None, 0, None, ctypes.byref(ctypes.c_void_p())) == L.ERR_VALUE
-    # precision modes: an unknown one is refused; float64 window sums are single-view only
+    # precision modes: an unknown one is refused; float64 and compensated window sums are
+    # single-view only, and the compensated ones need constant planes
     b = L.SweepArgs()
-    b.n_src, b.r, b.top_k, b.geo, b.precision = 1, 1, 1, geo.ctypes.data, 3
+    b.n_src, b.r, b.top_k, b.geo, b.precision = 1, 1, 1, geo.ctypes.data, 5
     assert lib.mvs_sweep(ctypes.addressof(b), None) == L.ERR_VALUE
     assert "unknown precision" in L.last_error()
     h = ctypes.c_void_p()
     assert lib.mvs_server_create(4, 4, 3, L.PREC_FP64_SUMS, ctypes.byref(h)) == L.ERR_UNSUPPORTED
+    assert lib.mvs_server_create(4, 4, 3, L.PREC_FP16_COMP, ctypes.byref(h)) == L.ERR_UNSUPPORTED
     assert "single-view" in L.last_error()
     jobs = (L.BatchJob * 1)()
     j = jobs[0].sweep
