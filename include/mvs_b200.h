@@ -462,6 +462,13 @@ mvs_status mvs_device_faults(uint32_t* count);
  * after it, from any thread. No counterpart in the reference. */
 uint32_t mvs_set_wait_limit(uint32_t iterations);
 
+/* Bounds-checked debug build only (libmvs_b200_debug.so, compiled with MVS_DEBUG_BOUNDS): the
+ * number of shared-memory and global indices the tile engine, the batched kernels and PatchMatch
+ * used outside their buffers since the last call (synchronises; clears the counts). Release
+ * builds return MVS_ERR_UNSUPPORTED. No counterpart in the reference (its Cython kernels are
+ * compiled with boundscheck=False). */
+mvs_status mvs_debug_bound_violations(uint32_t* count);
+
 /* Message of this thread's last failing call ("" if none). Returns the message length. */
 size_t mvs_last_error(char* buf, size_t cap);
 /* Library version string. */

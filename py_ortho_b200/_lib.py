@@ -15,7 +15,10 @@ import numpy as np
 import torch
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libmvs_b200.so")
+# MVS_LIBRARY=debug-bounds loads the bounds-checked debug build (python -m py_ortho_b200.build
+# --debug-bounds) instead of the release library
+LIB_PATH = os.path.join(HERE, "libmvs_b200_debug.so" if os.environ.get("MVS_LIBRARY") == "debug-bounds"
+                        else "libmvs_b200.so")
 
 MAX_SOURCES = 16
 MAX_RADIUS = 7
@@ -133,6 +136,7 @@ SIGNATURES = {
     "mvs_last_error": (C.c_size_t, [C.c_char_p, C.c_size_t]),
     "mvs_device_faults": (i32, [vp]),
     "mvs_set_wait_limit": (C.c_uint32, [C.c_uint32]),
+    "mvs_debug_bound_violations": (i32, [vp]),
     "mvs_version": (C.c_char_p, []),
 }
 

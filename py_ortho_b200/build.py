@@ -44,8 +44,13 @@ def _stale(target: str, deps: list[str]) -> bool:
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, debug_bounds: bool = False) -> str:
+    """Compiles the library; debug_bounds: the bounds-checked build (-DMVS_DEBUG_BOUNDS) into
+    libmvs_b200_debug.so, objects under _build/debug."""
+    build_dir = os.path.join(BUILD, "debug") if debug_bounds else BUILD
+    lib = LIB.replace("libmvs_b200.so", "libmvs_b200_debug.so") if debug_bounds else LIB
+    flags = ["-DMVS_DEBUG_BOUNDS"] if debug_bounds else []
+    os.makedirs(build_dir, exist_ok=True)
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
     headers.append(os.path.join(INCLUDE, "mvs_b200.h"))
     objs = []
@@ -54,10 +59,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         path = os.path.join(CSRC, src)
         if not os.path.exists(path):
             continue
-        obj = os.path.join(BUILD, src.replace(".cu", ".o"))
+        obj = os.path.join(build_dir, src.replace(".cu", ".o"))
         objs.append(obj)
         if force or ptxas_info or _stale(obj, [path] + headers):
-            cmd = [cc, "-c", path, "-o", obj] + ARCH + COMMON + EXTRA.get(src, [])
+            cmd = [cc, "-c", path, "-o", obj] + ARCH + COMMON + EXTRA.get(src, []) + flags
             if ptxas_info:
                 cmd += ["-Xptxas", "-v"]
             if verbose:
@@ -67,14 +72,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
                 raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
             if ptxas_info or verbose:
                 sys.stdout.write(r.stdout + r.stderr)
-    if force or _stale(LIB, objs):
-        cmd = [cc, "-shared", "-o", LIB] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+    if force or _stale(lib, objs):
+        cmd = [cc, "-shared", "-o", lib] + objs + ARCH + ["-Xcompiler", "-fPIC"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
-    return LIB
+    return lib
 
 
 def main(argv=None) -> int:
@@ -82,8 +87,10 @@ def main(argv=None) -> int:
     ap.add_argument("--force", action="store_true")
     ap.add_argument("--verbose", action="store_true")
     ap.add_argument("--ptxas-info", action="store_true", help="print registers / spills per kernel")
+    ap.add_argument("--debug-bounds", action="store_true",
+                    help="the bounds-checked debug build (libmvs_b200_debug.so)")
     a = ap.parse_args(argv)
-    print(build(a.force, a.verbose, a.ptxas_info))
+    print(build(a.force, a.verbose, a.ptxas_info, a.debug_bounds))
     return 0
 
 

@@ -509,3 +509,5 @@ extern "C" mvs_status mvs_server_step(mvs_server* s, const int32_t* slots, const
 }
 
 extern "C" void mvs_server_destroy(mvs_server* s) { server_free(s); }
+
+unsigned mvs::take_bound_violations_batch() { return take_bound_violations_here(); }

@@ -58,6 +58,36 @@ inline int num_sms() {
     return n;
 }
 
+// Bounds-checked debug build (nvcc -DMVS_DEBUG_BOUNDS; `python -m py_ortho_b200.build
+// --debug-bounds` writes libmvs_b200_debug.so): MVS_BOUND(cond) counts every shared-memory or
+// global index the instrumented kernels (tile engine, batched / server kernels, PatchMatch) would
+// use outside its buffer, in a per-translation-unit device counter that the host reads with
+// mvs_debug_bound_violations. The access itself still happens (the counter records, it does not
+// trap), so tests run the debug build on small cases only. Release builds compile the checks away.
+#ifdef MVS_DEBUG_BOUNDS
+static __device__ unsigned g_bound_violations;
+#define MVS_BOUND(cond)                                                  \
+    do {                                                                 \
+        if (!(cond)) atomicAdd(&::mvs::g_bound_violations, 1u);          \
+    } while (0)
+// host: this translation unit's count, cleared
+static inline unsigned take_bound_violations_here() {
+    unsigned n = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&n, g_bound_violations, sizeof(n)) != cudaSuccess) return ~0u;
+    cudaMemcpyToSymbol(g_bound_violations, &zero, sizeof(zero));
+    return n;
+}
+#else
+#define MVS_BOUND(cond) \
+    do {                \
+    } while (0)
+static inline unsigned take_bound_violations_here() { return 0; }
+#endif
+// per-unit readers (sweep.cu, batch.cu, patchmatch.cu), summed by mvs_debug_bound_violations
+unsigned take_bound_violations_sweep();
+unsigned take_bound_violations_batch();
+unsigned take_bound_violations_pm();
+
 // NaN-propagating max with a float32 floor (np.maximum semantics).
 __device__ __forceinline__ float max_nan(float v, float lo) { return (v >= lo || v != v) ? v : lo; }
 __device__ __forceinline__ double max_nan(double v, double lo) { return (v >= lo || v != v) ? v : lo; }

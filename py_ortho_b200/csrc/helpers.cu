@@ -471,3 +471,16 @@ extern "C" mvs_status mvs_depth_band(const mvs_depth_band_args* a, void* stream)
     if (cells) cudaFreeAsync(cells, st);
     return s;
 }
+
+extern "C" mvs_status mvs_debug_bound_violations(uint32_t* count) {
+    clear_error();
+#ifdef MVS_DEBUG_BOUNDS
+    MVS_CUDA(cudaDeviceSynchronize(), "debug bounds: synchronise");
+    const unsigned n = take_bound_violations_sweep() + take_bound_violations_batch() + take_bound_violations_pm();
+    if (count) *count = n;
+    return MVS_OK;
+#else
+    if (count) *count = 0;
+    return fail(MVS_ERR_UNSUPPORTED, "this library was built without bounds checks (MVS_DEBUG_BOUNDS)");
+#endif
+}

@@ -45,6 +45,7 @@ struct PMParams {
     double* pbest;                     // cost of the plane kept by propagation
     double* psc;                       // its photo score
     const unsigned* pstate;            // xorshift32 state before the pixel's first draw
+    unsigned win_smem;                 // dynamic shared bytes of the lane kernel (bounds checks)
     const float* img[MVS_MAX_SOURCES];
     const float* dep[MVS_MAX_SOURCES];
     int iw[MVS_MAX_SOURCES], ih[MVS_MAX_SOURCES];
@@ -220,6 +221,7 @@ __device__ double pm_cost(const PMParams& c, int y, int x, double d, const doubl
                         const double us = in ? u : 0.0, vs = in ? v : 0.0;
                         const int x0 = (int)us, y0 = (int)vs;
                         const double fx = us - (double)x0, fy = vs - (double)y0;
+                        MVS_BOUND((long long)y0 * iw + x0 >= 0 && (long long)y0 * iw + x0 + iw + 1 < (long long)iw * ih);
                         const float* im = c.img[s] + ((long long)y0 * iw + x0);
                         const double a00 = __ldg(im), a01 = __ldg(im + 1), a10 = __ldg(im + iw), a11 = __ldg(im + iw + 1);
                         const double J = (a00 * (1.0 - fx) + a01 * fx) * (1.0 - fy) + (a10 * (1.0 - fx) + a11 * fx) * fy;
@@ -583,6 +585,7 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
         const int yi = pmf_floor(vl, fv) + vb + 0x4B400000;
         // the clamp keeps every tap inside the image whatever the inputs
         const int o = min(max(yi * sw + xi, 0), last);
+        MVS_BOUND(o >= 0 && o <= last);
         const float fx = ul - fu, fy = vl - fv;
         const float* t = im + o;
         const float t00 = __ldg(t), t01 = __ldg(t + 1), t10 = __ldg(t + sw), t11 = __ldg(t + sw + 1);
@@ -865,6 +868,7 @@ __global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const 
     const int side = NSIDE > 0 ? NSIDE : pm_side(c.r, c.step);
     const int nw = side * side;
     float4* win = pm_win + (threadIdx.x / L) * (nw + 4);
+    MVS_BOUND((threadIdx.x / L + 1) * (nw + 4) * sizeof(float4) <= c.win_smem);
     const float rpx = __ldg(c.ray + idx), rpy = __ldg(c.ray + HW + idx), rpz = __ldg(c.ray + 2 * HW + idx);
     PMWin wn;
     wn.w = win;
@@ -1156,6 +1160,7 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     while (groups > 1 && (size_t)groups * win_bytes > 96 * 1024) groups >>= 1;
     const int block = fast ? groups * lanes : 128;
     const size_t smem = fast ? (size_t)groups * win_bytes : 0;
+    p.win_smem = (unsigned)smem;
     void (*lane_kernel[2])(PMParams) = {nullptr, nullptr};
     mvs_status status = MVS_OK;
     if (fast) {
@@ -1202,3 +1207,5 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     cudaFreeAsync(scratch, st);
     return status;
 }
+
+unsigned mvs::take_bound_violations_pm() { return take_bound_violations_here(); }

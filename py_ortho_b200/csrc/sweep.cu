@@ -403,3 +403,5 @@ extern "C" mvs_status mvs_device_faults(uint32_t* count) {
     if (count) *count = n;
     return n ? fail(MVS_ERR_TIMEOUT, "%u sweep tile(s) gave up waiting for their reference copy", n) : MVS_OK;
 }
+
+unsigned mvs::take_bound_violations_sweep() { return take_bound_violations_here(); }

@@ -181,6 +181,7 @@ __device__ __forceinline__ float sample_plane(const Coef& c, const void* img, in
     // integer guard: every tap stays inside the image whatever the float rounding did
     ok = ok && (unsigned)x0 < (unsigned)(w - 1) && (unsigned)y0 < (unsigned)(h - 1);
     const long long o = ok ? (long long)y0 * w + x0 : 0;
+    MVS_BOUND(o >= 0 && o + w + 1 < (long long)h * w);
     const float fx = ul - fu, fy = vl - fv;
     const float a00 = tap<F16>(img, o), a01 = tap<F16>(img, o + 1);
     const float a10 = tap<F16>(img, o + w), a11 = tap<F16>(img, o + w + 1);
@@ -206,6 +207,7 @@ __device__ __forceinline__ float sample_plane_inside(const Coef& c, const void* 
     // geometry defeated that test (unsigned arithmetic: wrap-around is defined and is clamped too)
     const unsigned xi = (unsigned)(c.U0 + floor_fma(ul, fu)), yi = (unsigned)(c.V0 + floor_fma(vl, fv));
     const unsigned o = min(yi * (unsigned)w + xi, (unsigned)(h - 1) * (unsigned)w - 2u);
+    MVS_BOUND((unsigned long long)o + w + 1 < (unsigned long long)h * w);
     const float fx = ul - fu, fy = vl - fv;
     const float a00 = tap<F16>(img, o), a01 = tap<F16>(img, o + 1);
     const float a10 = tap<F16>(img, o + w), a11 = tap<F16>(img, o + w + 1);
@@ -235,6 +237,7 @@ __device__ __forceinline__ float sample_ray(const SweepParams& p, const SrcGeo& 
     const int x0 = (int)u, y0 = (int)v;
     const double fx = u - (double)x0, fy = v - (double)y0;
     const long long so = (long long)y0 * g.w + x0;
+    MVS_BOUND(so >= 0 && so + g.w + 1 < (long long)g.h * g.w);
     const double a00 = tap<false>(g.img, so), a01 = tap<false>(g.img, so + 1);
     const double a10 = tap<false>(g.img, so + g.w), a11 = tap<false>(g.img, so + g.w + 1);
     const double val = (a00 * (1.0 - fx) + a01 * fx) * (1.0 - fy) + (a10 * (1.0 - fx) + a11 * fx) * fy;
@@ -307,6 +310,7 @@ __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4
     // consecutive threads take consecutive rows of one segment: a quarter-warp's 16-byte loads then
     // start (19 hy + 4 sg) mod 8 float4 units into the bank space - 8 distinct groups (JP = 76)
     const int sg = tid / HR, hy = tid - sg * HR;
+    MVS_BOUND(hy < HR && P * sg + P <= TW && hy * JP + P * sg + NIN <= HR * JP);
     const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
     const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
     float v[NIN], s1[NIN], s2[NIN], s3[NIN];
@@ -365,6 +369,7 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
+    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
     float cv = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
 #pragma unroll
     for (int t = 0; t < K; ++t) {
@@ -423,6 +428,7 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
     const int sg = tid / HR, hy = tid - sg * HR;
+    MVS_BOUND(hy < HR && P * sg + P <= TW && hy * JP + P * sg + NIN <= HR * JP);
     const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
     const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
     float v[NIN], jz[NIN], q2[NIN], q3[NIN];
@@ -479,6 +485,7 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
+    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
     float cv = 0.f;
     double cj = 0.0, cjj = 0.0, cji = 0.0;
 #pragma unroll
@@ -547,6 +554,7 @@ __device__ __forceinline__ void stage_b_cmp(const float* sJ, const float* sI, fl
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
     const int sg = tid / HR, hy = tid - sg * HR;
+    MVS_BOUND(hy < HR && P * sg + P <= TW && hy * JP + P * sg + NIN <= HR * JP);
     const float4* jr = reinterpret_cast<const float4*>(sJ + hy * JP + P * sg);
     const float4* ir = reinterpret_cast<const float4*>(sI + hy * JP + P * sg);
     float v[NIN], s0[NIN], s1[NIN], s2[NIN], s3[NIN];
@@ -621,6 +629,7 @@ __device__ __forceinline__ void stage_c_cmp(const float4* sH, const unsigned cha
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
+    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
     const unsigned char* ccol = sV + y0 * TW + c;
     float cv = 0.f, ci = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
     float ej = 0.f, ejj = 0.f, eji = 0.f;            // Kahan compensations
@@ -930,6 +939,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
 #pragma unroll
                     for (int k = 0; k < MR; ++k) {
                         if ((k + 1) * SEG <= HR || seg + k * SEG < HR) {
+                            MVS_BOUND((seg + k * SEG) * JP + (RA - R) + c < HR * JP);
                             any_invalid |= Jv[k] != Jv[k];
                             col[k * SEG * JP] = CMP ? __fsub_rn(Jv[k], pv) : Jv[k];
                         }
@@ -939,6 +949,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                         const int e0 = tid + m * NT;
                         if (e0 < XS) {
                             const int hy = e0 / XW, hc = TW + (e0 - hy * XW);
+                            MVS_BOUND(hy * JP + (RA - R) + hc < HR * JP);
                             any_invalid |= Jv[MR + m] != Jv[MR + m];
                             sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(Jv[MR + m], pv) : Jv[MR + m];
                         }
@@ -950,6 +961,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                         if (e < HR * HC) {
                             const int hy = e / HC, hc = e - hy * HC;
                             const float J = sample_plane_inside<F16>(cf, img, sw, sh, (float)hc, (float)hy);
+                            MVS_BOUND(hy * JP + (RA - R) + hc < HR * JP);
                             any_invalid |= J != J;
                             sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(J, pv) : J;
                         }
@@ -963,6 +975,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
                             const int gy = ty - R + hy, gxx = tx - R + hc;
                             const bool in = gy >= 0 && gy < H && gxx >= 0 && gxx < W;
                             const float J = sample_plane<F16>(cf, img, sw, sh, (float)hc, (float)hy, in);
+                            MVS_BOUND(hy * JP + (RA - R) + hc < HR * JP);
                             any_invalid |= J != J;
                             sJ[hy * JP + (RA - R) + hc] = CMP ? __fsub_rn(J, pv) : J;
                         }
@@ -1030,6 +1043,7 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             if (bottom) sc = __fsub_rn(total[j], sc);
             sc = __fdiv_rn(sc, (float)kk);
             const int w = (seg * ROWS + j) * TW + c;
+            MVS_BOUND(w < TH * TW);
             float best = sW[w], prv = sW[TH * TW + w];
             const int id = __float_as_int(sW[5 * TH * TW + w]);
             if (id == i - 1) sW[3 * TH * TW + w] = sc;
