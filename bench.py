@@ -200,7 +200,8 @@ def run_ours(a):
         state[4].fill_(-1)
         if timed:
             ev["sweep"][0].record(stream)
-        L.check(lib.mvs_sweep(ctypes.addressof(a_sw), sh), "sweep")
+        with L.nvtx("sweep"):
+            L.check(lib.mvs_sweep(ctypes.addressof(a_sw), sh), "sweep")
         if timed:
             ev["sweep"][1].record(stream)
         h = hyp.c()
@@ -211,7 +212,8 @@ def run_ours(a):
             score.zero_()
             if timed:
                 ev["pm"][0].record(stream)
-            L.check(lib.mvs_pm_refine(ctypes.addressof(pm), sh), "pm_refine")
+            with L.nvtx("patchmatch"):
+                L.check(lib.mvs_pm_refine(ctypes.addressof(pm), sh), "pm_refine")
             if timed:
                 ev["pm"][1].record(stream)
         if timed:

@@ -7,6 +7,7 @@ RuntimeError).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import threading
@@ -184,6 +185,22 @@ def check(status: int, what: str = "") -> None:
     if status == ERR_UNSUPPORTED:
         raise NotImplementedError(msg)
     raise RuntimeError(msg)
+
+
+@contextlib.contextmanager
+def nvtx(name: str):
+    """An NVTX range around a phase of the host drivers (visible to Nsight Systems / ncu's NVTX
+    filters); a no-op where NVTX is unavailable."""
+    try:
+        torch.cuda.nvtx.range_push(name)
+        pushed = True
+    except Exception:      # noqa: BLE001 - profiling aid only
+        pushed = False
+    try:
+        yield
+    finally:
+        if pushed:
+            torch.cuda.nvtx.range_pop()
 
 
 def check_device_faults() -> None:

@@ -292,7 +292,13 @@ def depth_map(k, nbrs, rec, views, opt: DepthOptions):
 
 def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
     """depth_map with its results left on the device: (depth, score, low_texture) tensors, or None."""
-    rng = _depth_range(rec, k)
+    with L.nvtx(f"depth_map view {k}"):
+        return _depth_map_device(k, nbrs, rec, views, opt)
+
+
+def _depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
+    with L.nvtx("depth range"):
+        rng = _depth_range(rec, k)
     if rng is None or not nbrs:
         return None
     ref, _, cam_r = views(k)
@@ -316,9 +322,11 @@ def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
         rays.append(fast.half(rays[-1][:, :2 * h, :2 * w].contiguous()))
     nd = _num_depths(rec, k, nbrs, rng, pyr_c[lv].f, opt.num_depths)
     shape = tuple(pyr_r[lv].shape)
-    base_t, step_t, _ = _band_maps(rec, k, pyr_c[lv], shape, rng, nd, block=max(8, shape[1] // 16))
-    d, _, _, _ = sweep_device(pyr_r[lv], pyr_c[lv], pyr_s[lv], pyr_cs[lv], Hypotheses.linear(base_t, step_t, nd),
-                              opt, rays[lv], precision=_per_pixel_precision(opt))
+    with L.nvtx("tie-point band"):
+        base_t, step_t, _ = _band_maps(rec, k, pyr_c[lv], shape, rng, nd, block=max(8, shape[1] // 16))
+    with L.nvtx(f"coarse sweep {nd} hypotheses"):
+        d, _, _, _ = sweep_device(pyr_r[lv], pyr_c[lv], pyr_s[lv], pyr_cs[lv], Hypotheses.linear(base_t, step_t, nd),
+                                  opt, rays[lv], precision=_per_pixel_precision(opt))
     dstep = step_t / 2
     score = sd = None
     for lvl in range(lv - 1, -1, -1):
@@ -326,9 +334,10 @@ def depth_map_device(k, nbrs, rec, views, opt: DepthOptions):
         up = _upsample2(d, H, W)
         dstep = _upsample2(dstep, H, W)
         iu = (1.0 / up).contiguous()
-        d, score, sd, _ = sweep_device(pyr_r[lvl], pyr_c[lvl], pyr_s[lvl], pyr_cs[lvl],
-                                       Hypotheses.refine(iu, dstep, opt.refine_steps), opt, rays[lvl],
-                                       precision=_per_pixel_precision(opt))
+        with L.nvtx(f"refine level {lvl}"):
+            d, score, sd, _ = sweep_device(pyr_r[lvl], pyr_c[lvl], pyr_s[lvl], pyr_cs[lvl],
+                                           Hypotheses.refine(iu, dstep, opt.refine_steps), opt, rays[lvl],
+                                           precision=_per_pixel_precision(opt))
         dstep = dstep / 2
     mask = torch.from_numpy(ref_mask).to(d.device)
     depth = torch.where(mask | (d < rng[0]) | (d > rng[1]), torch.full_like(d, float("nan")), d)

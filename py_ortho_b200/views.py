@@ -326,7 +326,8 @@ def densify_views(rec, views, opt: DepthOptions, nbrs: Optional[List[List[int]]]
     extra: Dict[int, tuple] = {}
 
     def pass1(k):
-        r = depth_map_device(k, nbrs[k], rec, views, opt)
+        with L.nvtx(f"pass 1 view {k}"):
+            r = depth_map_device(k, nbrs[k], rec, views, opt)
         if r is None:
             return None
         depth, score, low = r
@@ -335,7 +336,8 @@ def densify_views(rec, views, opt: DepthOptions, nbrs: Optional[List[List[int]]]
 
     def pass2(k, maps):
         score, low = extra[k]
-        D, ch, na = repair(k, maps, score, low, views, nbrs[k], rec, settings, opt)
+        with L.nvtx(f"pass 2 view {k}"):
+            D, ch, na = repair(k, maps, score, low, views, nbrs[k], rec, settings, opt)
         torch.cuda.current_stream().synchronize()
         L.check_device_faults()      # a sweep tile of pass 1 or 2 that gave up raises here
         return D.cpu().numpy(), ch, na
