@@ -252,32 +252,47 @@ def assign_views(costs: Sequence[float], world: int) -> List[int]:
 
 def wanted_maps(owner: Sequence[int], nbrs: Sequence[Sequence[int]], have: Sequence[int]) -> List[int]:
     """Views whose pass-1 map a view on another rank uses, in view order."""
+    return sorted(map_destinations(owner, nbrs, have))
+
+
+def map_destinations(owner: Sequence[int], nbrs: Sequence[Sequence[int]], have: Sequence[int]) -> Dict[int, List[int]]:
+    """For every pass-1 map that views on other ranks read: the ranks that read it (sorted)."""
     hv = set(have)
-    out = set()
+    out: Dict[int, set] = {}
     for k, nb in enumerate(nbrs):
         if k not in hv:
             continue
         for j in nb:
             if j in hv and owner[j] != owner[k]:
-                out.add(j)
-    return sorted(out)
+                out.setdefault(j, set()).add(owner[k])
+    return {j: sorted(r) for j, r in out.items()}
 
 
 def exchange_maps(local: Dict[int, torch.Tensor], owner: Sequence[int], shapes: Dict[int, tuple],
-                  send: Sequence[int], rank: int, group=None, device=None) -> Dict[int, torch.Tensor]:
-    """Every map in ``send`` is broadcast from its owner to all ranks (in view order, so every rank
-    issues the same collectives). Returns ``local`` plus the maps received."""
+                  dests: Dict[int, List[int]], rank: int, group=None, device=None) -> Dict[int, torch.Tensor]:
+    """Point to point: each map goes from its owner to the ranks whose views read it, and to no
+    other rank. Every rank walks the maps in view order, so the sends and receives between any two
+    ranks pair up in the same order. Returns ``local`` plus the maps received."""
     import torch.distributed as dist
     out = dict(local)
-    for j in send:
+    reqs = []
+    for j in sorted(dests):
         if owner[j] == rank:
             buf = local[j].contiguous()
-        else:
+            for dst in dests[j]:
+                reqs.append(dist.isend(buf, dst=_global_rank(dst, group), group=group))
+        elif rank in dests[j]:
             buf = torch.empty(shapes[j], dtype=torch.float32, device=device)
-        dist.broadcast(buf, src=owner[j], group=group)
-        if owner[j] != rank:
+            reqs.append(dist.irecv(buf, src=_global_rank(owner[j], group), group=group))
             out[j] = buf
+    for q in reqs:
+        q.wait()
     return out
+
+
+def _global_rank(r: int, group) -> int:
+    import torch.distributed as dist
+    return r if group is None else dist.get_global_rank(group, r)
 
 
 def run_passes(n_views: int, nbrs: Sequence[Sequence[int]], costs: Sequence[float], shapes: Dict[int, tuple],
@@ -306,7 +321,7 @@ def run_passes(n_views: int, nbrs: Sequence[Sequence[int]], costs: Sequence[floa
     have = [k for k, f in enumerate(flags.tolist()) if f]
     maps = local
     if world > 1:
-        maps = exchange_maps(local, owner, shapes, wanted_maps(owner, nbrs, have), rank, group, device)
+        maps = exchange_maps(local, owner, shapes, map_destinations(owner, nbrs, have), rank, group, device)
     return {k: pass2(k, maps) for k in mine if k in local}
 
 

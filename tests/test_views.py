@@ -86,6 +86,8 @@ def test_wanted_maps():
     assert V.wanted_maps(owner, nbrs, have=[0, 1, 2, 3]) == [0, 1, 2, 3]
     assert V.wanted_maps(owner, nbrs, have=[0, 2, 3]) == [2, 3]
     assert V.wanted_maps([0, 0, 0, 0], nbrs, have=[0, 1, 2, 3]) == []
+    # each map goes only to the ranks whose views read it
+    assert V.map_destinations([0, 1, 2, 1], [[1], [0], [1], []], have=[0, 1, 2, 3]) == {0: [1], 1: [0, 2]}
 
 
 # ------------------------------------------------------------------ sharded orchestration on gloo
@@ -134,20 +136,23 @@ def _free_port():
     return p
 
 
-def test_run_passes_two_ranks_gloo_matches_one_rank():
+@pytest.mark.parametrize("world", [2, 3])
+def test_run_passes_on_gloo_ranks_matches_one_rank(world):
+    """Passes 1 and 2 sharded over 2 and 3 gloo ranks: every view's pass 2 sees exactly the maps a
+    single process gives it (each map sent point to point to the ranks that read it)."""
     single = V.run_passes(N_VIEWS, NBRS, COSTS, SHAPES, _pass1, _pass2, device=torch.device("cpu"))
     assert sorted(single) == [k for k in range(N_VIEWS) if k != NO_MAP]
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _free_port()
-    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_worker, args=(r, world, port, q)) for r in range(world)]
     for p in procs:
         p.start()
     res = dict(q.get(timeout=120) for _ in procs)
     for p in procs:
         p.join(60)
         assert p.exitcode == 0
-    owner = V.assign_views(COSTS, 2)
+    owner = V.assign_views(COSTS, world)
     merged = {}
     for rank, out in res.items():
         assert all(owner[k] == rank for k in out)                   # each view on its owner only
