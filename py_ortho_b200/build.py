@@ -73,12 +73,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, 
             if ptxas_info or verbose:
                 sys.stdout.write(r.stdout + r.stderr)
     if force or _stale(lib, objs):
-        cmd = [cc, "-shared", "-o", lib] + objs + ARCH + ["-Xcompiler", "-fPIC"]
+        tmp = lib + ".partial"              # linked aside, then moved into place in one step
+        cmd = [cc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")
+        os.replace(tmp, lib)
     return lib
 
 

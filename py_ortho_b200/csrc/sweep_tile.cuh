@@ -244,17 +244,37 @@ __device__ __forceinline__ float sample_ray(const SweepParams& p, const SrcGeo& 
     return isfinite(val) ? (float)val : qnan();
 }
 
-__device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, int oy, int hc_span, int hr_span) {
+// The plane map of one (hypothesis, source, tile), composed in FP64 and rounded once (Coef),
+// by the 4 lanes of an aligned lane group: lane k tests corner k of the halo rectangle, lane 0
+// also forms the map, so the four corner tests' divisions run in parallel. A projective map whose
+// depth stays positive maps the halo rectangle onto the convex hull of its corner images, so four
+// corners strictly inside (a 1e-3 px margin absorbs the FP32 evaluation error of ~1e-5 px) put
+// every sample inside. Every lane of the calling warps must call it (width-4 shuffles); `write`
+// selects the groups that store their source's Coef.
+__device__ inline void make_coef_group(Coef& c, const SrcGeo& g, float inv, int ox, int oy, int hc_span, int hr_span,
+                                       bool write) {
+    const int k = threadIdx.x & 3;
     const double d = 1.0 / (double)inv;
     double g0[3], g1[3], g2[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        g1[k] = d * g.m[3 * k + 0];
-        g2[k] = d * g.m[3 * k + 1];
-        g0[k] = d * (g.m[3 * k + 0] * (double)ox + g.m[3 * k + 1] * (double)oy + g.m[3 * k + 2]) + g.b[k];
+    for (int q = 0; q < 3; ++q) {
+        g1[q] = d * g.m[3 * q + 0];
+        g2[q] = d * g.m[3 * q + 1];
+        g0[q] = d * (g.m[3 * q + 0] * (double)ox + g.m[3 * q + 1] * (double)oy + g.m[3 * q + 2]) + g.b[q];
     }
     const double Z0 = g0[2];
     const bool norm = fabs(Z0) > 1e-9;
+    // corner k of the halo rectangle: (0, 0), (w - 1, 0), (0, h - 1), (w - 1, h - 1)
+    const double ca = (k & 1) ? (double)(hc_span - 1) : 0.0, cb = (k & 2) ? (double)(hr_span - 1) : 0.0;
+    const double Xc = g0[0] + ca * g1[0] + cb * g2[0];
+    const double Yc = g0[1] + ca * g1[1] + cb * g2[1];
+    const double Zc = g0[2] + ca * g1[2] + cb * g2[2];
+    const double uc = g.f * Xc / Zc + g.cx, vc = g.f * Yc / Zc + g.cy;
+    int in = Zc > 1e-5 && uc >= 1e-3 && vc >= 1e-3 && uc <= (double)g.w - 1.001 - 1e-3 &&
+             vc <= (double)g.h - 1.001 - 1e-3;
+    in &= __shfl_xor_sync(0xffffffffu, in, 1, 4);
+    in &= __shfl_xor_sync(0xffffffffu, in, 2, 4);
+    if (k != 0 || !write) return;
     const double zs = norm ? Z0 : 1.0;
     const double rzs = 1.0 / zs;
     double U0 = 0.0, V0 = 0.0;
@@ -280,23 +300,7 @@ __device__ inline void make_coef(Coef& c, const SrcGeo& g, float inv, int ox, in
     c.hi_v = (float)(((double)g.h - 1.001) - V0);
     c.U0 = (int)U0;
     c.V0 = (int)V0;
-    // A projective map whose depth stays positive maps the halo rectangle onto the convex hull of
-    // its corner images, so four corners strictly inside (a 1e-3 px margin absorbs the FP32
-    // evaluation error of ~1e-5 px) put every sample inside.
-    bool inside = norm;
-    const double ca[2] = {0.0, (double)(hc_span - 1)}, cb[2] = {0.0, (double)(hr_span - 1)};
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const double Xc = g0[0] + ca[i] * g1[0] + cb[j] * g2[0];
-            const double Yc = g0[1] + ca[i] * g1[1] + cb[j] * g2[1];
-            const double Zc = g0[2] + ca[i] * g1[2] + cb[j] * g2[2];
-            const double uc = g.f * Xc / Zc + g.cx, vc = g.f * Yc / Zc + g.cy;
-            inside = inside && Zc > 1e-5 && uc >= 1e-3 && vc >= 1e-3 && uc <= (double)g.w - 1.001 - 1e-3 &&
-                     vc <= (double)g.h - 1.001 - 1e-3;
-        }
-    c.inside = inside ? 1 : 0;
+    c.inside = (norm && in) ? 1 : 0;
 }
 
 // Stage B: horizontal window sums of (V, J, J^2, J I) for one 16-column row segment per thread:
@@ -902,7 +906,11 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
         }
         if constexpr (PLANES) {
             __syncthreads();   // the previous hypothesis is done reading sC
-            if (tid < nsrc) make_coef(sC[tid], p.src[tid], p.planes[i - p.i0], tx - R, ty - R, HC, HR);
+            if (tid < 4 * MVS_MAX_SOURCES && (tid >> 5) * 8 < nsrc) {   // the warps that hold a source
+                const int sg_ = tid >> 2;
+                make_coef_group(sC[sg_ < nsrc ? sg_ : 0], p.src[sg_ < nsrc ? sg_ : 0], p.planes[i - p.i0], tx - R,
+                                ty - R, HC, HR, sg_ < nsrc);
+            }
         }
         for (int s = 0; s < nsrc; ++s) {
             __syncthreads();   // sC ready; the previous stage B is done with sJ
