@@ -252,6 +252,27 @@ def run_ours(a):
     value = world * evals * a.steps / (ms_total / 1e3)
     ms_sweep = acc["sweep"] / a.steps
     ms_pm = acc["pm"] / a.steps if iters else 0.0
+    # the other PatchMatch arithmetic, timed once after the timed region on the same state: the
+    # float64 kernel (the reference's arithmetic, bit-exact) when the step ran float32, or vice versa
+    pm_other = None
+    if iters and world == 1:
+        other = 0 if pm.precision == 1 else 1
+        keep_prec = pm.precision
+        pm.precision = other
+        ts_o = []
+        for rep in range(2):
+            normal.copy_(normal0)
+            score.zero_()
+            e0o, e1o = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0o.record(stream)
+            L.check(lib.mvs_pm_refine(ctypes.addressof(pm), sh), "pm_refine")
+            e1o.record(stream)
+            e1o.synchronize()
+            if rep:
+                ts_o.append(e0o.elapsed_time(e1o))
+        pm.precision = keep_prec
+        pm_other = {"precision": "fp64" if other == 0 else "fp32", "ms": round(ts_o[0], 3),
+                    "evals_per_s": pm_evals / (ts_o[0] / 1e3)}
     peaks = peaks_table()
     # sweep roofline: algorithmic bytes per evaluation (source pixel read once per plane, plus the
     # reference statistics and the winner state once per chunk)
@@ -296,6 +317,7 @@ def run_ours(a):
         "roofline": roof_sweep if dominant == "sweep" else dict(roof_sweep, note="pm dominates; see roofline_pm"),
         "roofline_pm": roof_pm,
         "phases_ms": {"sweep": round(ms_sweep, 3), "patchmatch": round(ms_pm, 3)},
+        "patchmatch_other_precision": pm_other,
         "clocks": clocks.summary(),
         "gpu_launches": launches * a.steps,
         "setup_s": round(setup_s, 1),
