@@ -261,6 +261,9 @@ def run_ours(a):
         pm.precision = other
         ts_o = []
         for rep in range(2):
+            h_ = hyp.c()                     # start from the sweep's depth, as the timed step does
+            L.check(lib.mvs_sweep_finalize(H, W, ctypes.addressof(h_), state[0].data_ptr(), state[2].data_ptr(),
+                                           state[3].data_ptr(), state[4].data_ptr(), depth.data_ptr(), sh))
             normal.copy_(normal0)
             score.zero_()
             e0o, e1o = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
