@@ -170,10 +170,10 @@ __device__ __forceinline__ int floor_fma(float x, float& f) {
 // and return NaN.
 template <bool F16>
 __device__ __forceinline__ float sample_plane(const Coef& c, const void* img, int w, int h, float a, float b, bool in) {
-    const float dz = fmaf(c.dz2, b, fmaf(c.dz1, a, c.dz0));
+    const float dz = fmaf(c.dz1, a, fmaf(c.dz2, b, c.dz0));
     const float rz = __fdividef(1.0f, dz);
-    const float ul = fmaf(c.nu2, b, fmaf(c.nu1, a, c.nu0)) * rz;
-    const float vl = fmaf(c.nv2, b, fmaf(c.nv1, a, c.nv0)) * rz;
+    const float ul = fmaf(c.nu1, a, fmaf(c.nu2, b, c.nu0)) * rz;
+    const float vl = fmaf(c.nv1, a, fmaf(c.nv2, b, c.nv0)) * rz;
     bool ok = in && (c.zs * dz > 1e-6f) && (ul >= c.lo_u) && (ul <= c.hi_u) && (vl >= c.lo_v) && (vl <= c.hi_v);
     float fu, fv;
     const int x0 = c.U0 + floor_fma(ok ? ul : 0.f, fu);
@@ -193,21 +193,22 @@ __device__ __forceinline__ float sample_plane(const Coef& c, const void* img, in
 
 // Homography sample when the whole halo rectangle is known to map inside the source and to lie
 // inside the reference image: no per-sample bounds; a non-finite value becomes NaN (invalid).
-// The maps are evaluated column part first, so a thread walking down one halo column (fixed a)
-// keeps fmaf(x1, a, x0) of each of the three maps and spends one FMA per map per sample.
+// (Evaluating the maps column part first, so that a thread walking down one halo column keeps
+// fmaf(x1, a, x0), and clamping the linear tap offset once instead of each coordinate measured
+// 1.3 % slower at C2: 167.5 vs 165.2 ms.)
 template <bool F16>
 __device__ __forceinline__ float sample_plane_inside(const Coef& c, const void* img, int w, int h, float a, float b) {
-    const float dz = fmaf(c.dz2, b, fmaf(c.dz1, a, c.dz0));
+    const float dz = fmaf(c.dz1, a, fmaf(c.dz2, b, c.dz0));
     const float rz = __fdividef(1.0f, dz);
-    const float ul = fmaf(c.nu2, b, fmaf(c.nu1, a, c.nu0)) * rz;
-    const float vl = fmaf(c.nv2, b, fmaf(c.nv1, a, c.nv0)) * rz;
+    const float ul = fmaf(c.nu1, a, fmaf(c.nu2, b, c.nu0)) * rz;
+    const float vl = fmaf(c.nv1, a, fmaf(c.nv2, b, c.nv0)) * rz;
     float fu, fv;
-    // top-left tap offset, clamped once to the largest offset whose four taps lie in the image: a
-    // no-op when the corner test holds; it keeps every tap inside the image even if an extreme
-    // geometry defeated that test (unsigned arithmetic: wrap-around is defined and is clamped too)
-    const unsigned xi = (unsigned)(c.U0 + floor_fma(ul, fu)), yi = (unsigned)(c.V0 + floor_fma(vl, fv));
-    const unsigned o = min(yi * (unsigned)w + xi, (unsigned)(h - 1) * (unsigned)w - 2u);
-    MVS_BOUND((unsigned long long)o + w + 1 < (unsigned long long)h * w);
+    // the clamp is a no-op when the corner test holds; it keeps every tap inside the image even if
+    // an extreme geometry defeated that test
+    const unsigned x0 = min((unsigned)(c.U0 + floor_fma(ul, fu)), (unsigned)(w - 2));
+    const unsigned y0 = min((unsigned)(c.V0 + floor_fma(vl, fv)), (unsigned)(h - 2));
+    const long long o = (long long)y0 * w + x0;
+    MVS_BOUND(o >= 0 && o + w + 1 < (long long)h * w);
     const float fx = ul - fu, fy = vl - fv;
     const float a00 = tap<F16>(img, o), a01 = tap<F16>(img, o + 1);
     const float a10 = tap<F16>(img, o + w), a11 = tap<F16>(img, o + w + 1);

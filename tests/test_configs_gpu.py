@@ -48,7 +48,13 @@ def _score_report(best, ref_best, same):
             "score_over_bar": int((e > SCORE_ABS).sum())}
 
 
-def test_c1_full_view_parity():
+@pytest.mark.parametrize("form", ["fp32", "fp64_sums"])
+def test_c1_full_view_parity(form):
+    """C1 in full, every pixel against the oracle. With the reference's own arithmetic for the
+    window sums (MVS_PREC_FP64_SUMS) the bar holds at every pixel. The default float32 sums meet it
+    on all but a stated handful of pixels at this small window (r = 2): bright low-texture windows
+    amplify their rounding ~1e3-fold (measured: 1 decided pixel of 307200 off by one plane)."""
+    from py_ortho_b200 import _lib as L
     from py_ortho_b200 import scene as S
     sc = S.make_scene("c1", seed=0, device="cuda")
     ref = sc.grey(sc.ref)
@@ -57,14 +63,16 @@ def test_c1_full_view_parity():
     assert (H, W, len(srcs)) == (480, 640, 4)
     planes = S.plane_list(35.0, 55.0, 128)
     r, top_k = 2, 2
-    st, depth, _, _, geo = _device_sweep(ref, srcs, sc, planes, r, top_k)
+    st, depth, _, _, geo = _device_sweep(ref, srcs, sc, planes, r, top_k,
+                                         L.PREC_FP64_SUMS if form == "fp64_sums" else L.PREC_FP32)
     ray = O.rays_world((H, W), sc.ref_cam)
     full = O.sweep(ref, srcs, ray, geo, [np.full((H, W), p, np.float32) for p in planes], r, top_k, keep_scores=True)
     idx, d, best = st[4].cpu().numpy(), depth.cpu().numpy(), st[0].cpu().numpy()
-    rep = check_parity(idx, d, None, full["idx"], full["depth"], None, gap_of(full["scores"]), "C1 640x480",
-                       flip_depth_frac=1e-4)
+    strict = form == "fp64_sums"
+    rep = check_parity(idx, d, None, full["idx"], full["depth"], None, gap_of(full["scores"]), f"C1 640x480 {form}",
+                       flip_depth_frac=0.0 if strict else 1e-4, decided_miss_frac=0.0 if strict else 2e-5)
     rep.update(_score_report(best, full["best"], idx == full["idx"]))
-    print("C1 parity:", rep)
+    print(f"C1 parity ({form}):", rep)
     assert rep["decided"] > 0.5 * H * W
 
 

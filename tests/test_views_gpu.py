@@ -79,10 +79,15 @@ def test_pass2_patchmatch_matches_reference():
     assert same_bits(Sg.cpu().numpy(), z[f"pm{k}_score_out"])
 
 
-def test_densify_views_end_to_end_against_reference():
-    """Passes 1 and 2 on the device against the reference's final depth maps. PatchMatch runs a
-    red-black schedule with counter-based draws where the reference visits pixels in raster order
-    with one xorshift stream, so repaired pixels agree statistically, not bit for bit."""
+@pytest.mark.parametrize("form", ["fp32", "fp64_sums"])
+def test_densify_views_end_to_end_against_reference(form):
+    """Passes 1 and 2 on the device against the reference's final depth maps. PatchMatch draws
+    from the reference's own stream, but which pixels draw (the active mask) follows pass 1, whose
+    float32 window sums decide a few near-threshold pixels the other way; one such pixel shifts the
+    stream for every pixel after it in raster order. With the reference's float64 window sums
+    (MVS_PREC_FP64_SUMS) pass 1 matches closely enough that >= 99.9 % of the final depths are
+    within 0.1 % of the reference's; with float32 sums, the stated weaker bar."""
+    from py_ortho_b200 import _lib as L
     from py_ortho_b200 import views as V
     from py_ortho_b200.densify import DepthOptions, _Cam
     z, rec, cams_ns, greys = views_fixture()
@@ -90,6 +95,8 @@ def test_densify_views_end_to_end_against_reference():
     opt = DepthOptions()
     opt.window, opt.num_depths = int(z["opt"][0]), int(z["opt"][1])
     opt.patchmatch = True
+    if form == "fp64_sums":
+        opt.precision = L.PREC_FP64_SUMS
 
     def views(k):
         return greys[k], None, cams[k]
@@ -101,13 +108,13 @@ def test_densify_views_end_to_end_against_reference():
         fin, rfin = np.isfinite(D), np.isfinite(ref)
         both = fin & rfin
         rel = np.abs(D[both].astype(np.float64) - ref[both]) / ref[both]
-        print(f"view {k}: finite agree {(fin == rfin).mean():.4f}, median rel {np.median(rel):.2e}, "
-              f"<=0.1% {(rel <= 1e-3).mean():.4f}, PM changes {ch}, active {na}")
+        print(f"{form} view {k}: finite agree {(fin == rfin).mean():.4f}, median rel {np.median(rel):.2e}, "
+              f"<=0.1% {(rel <= 1e-3).mean():.4f}, PM changes {ch}, active {na} (reference {int(z[f'pm{k}_active'].sum())})")
         ref_na = int(z[f"pm{k}_active"].sum())             # the mask follows pass 1's near-ties
         assert abs(na - ref_na) <= 0.05 * ref_na
         assert (fin == rfin).mean() > 0.95
         assert np.median(rel) < 1e-3
-        assert (rel <= 1e-3).mean() > 0.8
+        assert (rel <= 1e-3).mean() > (0.999 if form == "fp64_sums" else 0.85)
 
 
 @pytest.mark.parametrize("c", [0, 1])
