@@ -330,7 +330,7 @@ def test_fp64_sums_track_the_reference_at_every_pixel(sweep_cases):
                      f"fp64 sums case {H}x{W} n={c['n']} r={c['r']}")
         worst.append(e_max)
     print("fp64 sums, per-hypothesis score error max per case:", " ".join(f"{w:.1e}" for w in worst))
-    assert max(worst) <= 1e-5
+    assert max(worst) <= 2.5e-7          # measured 1.2e-7: one float32 ulp of the NCC, on one case
 
 
 def test_fp64_sums_meet_the_bar_at_every_pixel_on_planes():
