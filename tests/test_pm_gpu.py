@@ -205,3 +205,47 @@ def test_pm_fp32_cost_with_the_geometric_term():
     assert d.size > 0
     assert np.quantile(d, 0.999) <= 1e-5, f"99.9 % quantile {np.quantile(d, 0.999):.2e}"
     assert d.max() <= 1e-3, f"max {d.max():.2e}"
+
+
+@pytest.mark.parametrize("W,H,n_src,r,step,case", [(1, 9, 2, 2, 1, "plain"), (7, 1, 3, 1, 1, "plain"),
+                                                   (13, 11, 4, 3, 2, "plain"), (33, 17, 5, 2, 1, "no_active"),
+                                                   (29, 21, 3, 2, 1, "all_nan"), (31, 23, 6, 3, 1, "sparse"),
+                                                   (64, 40, 8, 3, 1, "plain")])
+def test_pm_stream_edge_cases_bit_exact_vs_oracle(W, H, n_src, r, step, case):
+    """The reference's stream on odd shapes (one-pixel rows and columns, odd widths whose colours
+    have unequal pixel counts), no active pixel (no draws at all), every depth NaN (pixels draw
+    only where a neighbour's plane was propagated in), and a sparse active mask: the float64 kernel
+    equals the oracle's sequential evaluation bit for bit, and the stream state left on the device
+    is the oracle's."""
+    from py_ortho_b200 import dense, scene as S
+    sc = S.make_scene("c2", seed=W + H, width=max(W, 8), height=max(H, 8))
+    ref = sc.grey(sc.ref)[:H, :W].astype(np.float32).copy()
+    srcs = [sc.grey(s).astype(np.float32) for s in sc.srcs[:n_src]]
+    rng = np.random.default_rng(W * 31 + H)
+    ray = O.rays_world((max(H, 8), max(W, 8)), sc.ref_cam)[:, :H, :W].copy()
+    par = np.array([c.row() for c in sc.src_cams[:n_src]], np.float64)
+    depth = (sc.depth_true[:H, :W] * (1 + rng.normal(0, 0.01, (H, W)))).astype(np.float32)
+    act = np.ones((H, W), np.uint8)
+    if case == "no_active":
+        act[:] = 0
+    elif case == "all_nan":
+        depth[:] = np.nan
+        depth[H // 2, W // 2] = sc.depth_true[H // 2, W // 2]
+    elif case == "sparse":
+        act = (rng.random((H, W)) < 0.2).astype(np.uint8)
+        depth[rng.random((H, W)) < 0.3] = np.nan
+    normal = S.tilted_normals(H, W, 3)
+    zr = float(sc.ref_cam.C[2])
+    args = (r, step, 2, 0.0, 0.02, 3, zr - 40.0, zr + 5.0, 2024)
+    a = [depth.copy(), normal.copy(), np.zeros((H, W), np.float32)]
+    b = [depth.copy(), normal.copy(), np.zeros((H, W), np.float32)]
+    st = dense.stream_start(2024)
+    ca = dense.pm_refine(ref, ray, sc.ref_cam.C, srcs, [None] * n_src, par, *a, act, *args, rng_state=st)
+    ost = np.array([2024 | 1], np.uint32)
+    cb = O.pm_refine(ref, ray, sc.ref_cam.C, srcs, [None] * n_src, par, *b, act, *args, state=ost)
+    assert ca == cb
+    for x, y in zip(a, b):
+        assert same_bits(x, y)
+    assert int(st.cpu().numpy().view(np.uint32)[0]) == int(ost[0])
+    if case == "no_active":
+        assert int(ost[0]) == 2024 | 1                 # nothing drew
