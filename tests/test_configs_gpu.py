@@ -48,12 +48,15 @@ def _score_report(best, ref_best, same):
             "score_over_bar": int((e > SCORE_ABS).sum())}
 
 
-@pytest.mark.parametrize("form", ["fp32", "fp64_sums"])
+@pytest.mark.parametrize("form", ["fp32", "fp64_sums_rays"])
 def test_c1_full_view_parity(form):
-    """C1 in full, every pixel against the oracle. With the reference's own arithmetic for the
-    window sums (MVS_PREC_FP64_SUMS) the bar holds at every pixel. The default float32 sums meet it
-    on all but a stated handful of pixels at this small window (r = 2): bright low-texture windows
-    amplify their rounding ~1e3-fold (measured: 1 decided pixel of 307200 off by one plane)."""
+    """C1 in full, every pixel against the oracle. With the reference's own arithmetic - float64
+    window sums (MVS_PREC_FP64_SUMS) on the per-pixel ray path (float64 projection and bilinear,
+    the 128 planes given as maps) - the bar holds at every pixel. The bench's path (float32 sums,
+    float32-evaluated homographies) meets it on all but a stated handful of pixels at this small
+    window (r = 2): bright low-texture windows amplify the float32 rounding ~1e3-fold (measured: 1
+    decided pixel of 307200 one plane off, 1 flipped pixel's depth 0.30 % off; float64 sums on the
+    homography path leave the same 1 decided pixel)."""
     from py_ortho_b200 import _lib as L
     from py_ortho_b200 import scene as S
     sc = S.make_scene("c1", seed=0, device="cuda")
@@ -63,12 +66,23 @@ def test_c1_full_view_parity(form):
     assert (H, W, len(srcs)) == (480, 640, 4)
     planes = S.plane_list(35.0, 55.0, 128)
     r, top_k = 2, 2
-    st, depth, _, _, geo = _device_sweep(ref, srcs, sc, planes, r, top_k,
-                                         L.PREC_FP64_SUMS if form == "fp64_sums" else L.PREC_FP32)
     ray = O.rays_world((H, W), sc.ref_cam)
+    if form == "fp32":
+        st, depth, _, _, geo = _device_sweep(ref, srcs, sc, planes, r, top_k, L.PREC_FP32)
+    else:
+        from py_ortho_b200 import dense, fast
+        geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+        ref_d = _dev(ref)
+        mu, sd = fast.ref_stats(ref_d, r)
+        maps = torch.from_numpy(np.repeat(planes.astype(np.float32)[:, None, None], H * W).reshape(-1, H, W)).cuda()
+        hyp = dense.Hypotheses(L.HYP_MAPS, len(planes), maps=maps)
+        st = dense.sweep(ref_d, mu, sd, _dev(ray), [_dev(s) for s in srcs], geo, hyp, r, top_k,
+                         precision=L.PREC_FP64_SUMS)
+        depth = dense.finalize(hyp, st)
+        torch.cuda.synchronize()
     full = O.sweep(ref, srcs, ray, geo, [np.full((H, W), p, np.float32) for p in planes], r, top_k, keep_scores=True)
     idx, d, best = st[4].cpu().numpy(), depth.cpu().numpy(), st[0].cpu().numpy()
-    strict = form == "fp64_sums"
+    strict = form != "fp32"
     rep = check_parity(idx, d, None, full["idx"], full["depth"], None, gap_of(full["scores"]), f"C1 640x480 {form}",
                        flip_depth_frac=0.0 if strict else 1e-4, decided_miss_frac=0.0 if strict else 2e-5)
     rep.update(_score_report(best, full["best"], idx == full["idx"]))
