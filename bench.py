@@ -39,7 +39,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--precision", choices=["fp32", "fp16"], default="fp32")
+    ap.add_argument("--precision", choices=["fp32", "fp16", "fp64sums"], default="fp32",
+                    help="window-sum / storage form of the sweep (fp64sums: the reference's float64 sums; "
+                         "--mode depthmap only)")
     ap.add_argument("--pm-precision", choices=["fp32", "fp64"], default="fp32",
                     help="PatchMatch cost arithmetic: fp32 windows (float64-composed homographies) or the "
                          "reference's float64 operation order (bit-exact)")
@@ -145,6 +147,8 @@ def run_ours(a):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
     L.load()
     cfg, W, H, nplanes, iters = workload(a)
+    if a.precision == "fp64sums":
+        raise SystemExit("--precision fp64sums applies to --mode depthmap")
     prec = L.PREC_FP16 if a.precision == "fp16" else L.PREC_FP32
     t0 = time.time()
     sc = S.make_scene(cfg, seed=rank, device=dev, width=W, height=H)
@@ -838,6 +842,9 @@ def run_depthmap(a):
     views = lambda k: (greys[k], None, dcams[k])         # host images, as densify's ImageCache hands them
     opt = Dn.DepthOptions()
     opt.window = cfg.radius
+    if a.precision == "fp64sums":
+        from py_ortho_b200 import _lib as L_
+        opt.precision = L_.PREC_FP64_SUMS
     nbrs = list(range(1, len(cams)))
     step = lambda: Dn.depth_map_device(0, nbrs, rec, views, opt)
     for _ in range(max(1, a.warmup)):
@@ -871,7 +878,8 @@ def run_depthmap(a):
             "config": {"workload": f"densify.depth_map on c2 {W}x{H}, {ns} sources, window {2 * cfg.radius + 1}, "
                                    f"num_depths {opt.num_depths}, refine_steps {opt.refine_steps}, 20000 tie points",
                        "path": "MVS_HYP_LINEAR coarse band + 2 x MVS_HYP_REFINE, float64 ray sampler; the "
-                               "step includes the host -> device copies of the 9 grey images"}}
+                               "step includes the host -> device copies of the 9 grey images",
+                       "window_sums": "float64 (the reference's)" if a.precision == "fp64sums" else "float32"}}
     print(json.dumps(line), flush=True)
 
 
