@@ -291,6 +291,15 @@ def run_ours(a):
                   "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": round(sweep_gbs / peaks["hbm_gbs"], 4),
                   "traffic": traffic, "peak_source": peaks["source"], "bytes_per_eval": round(bytes_per_eval, 4),
                   "evals_per_s": sweep_evals / (ms_sweep / 1e3), "ms": round(ms_sweep, 3)}
+    # the roof that binds this kernel: SIMT issue. 128 FP32 lanes x SMs x the sampled SM clock
+    # thread instructions per second, over the instructions per evaluation the committed ncu
+    # capture counts (profiles/sweep_kernel_3000x2250_8src_16planes.md)
+    n_sm = torch.cuda.get_device_properties(dev).multi_processor_count
+    clk = clocks.summary().get("sm_mhz") or 1965.0
+    issue_rate = 128.0 * n_sm * clk * 1e6
+    roof_sweep["issue_ceiling"] = {"thread_inst_per_s": issue_rate, "inst_per_eval_ncu": 159.0,
+                                   "ceiling_evals_per_s": issue_rate / 159.0,
+                                   "frac": round(roof_sweep["evals_per_s"] / (issue_rate / 159.0), 4)}
     roof_pm = None
     if iters:
         roof_pm = {"kernel": "pm_lane_kernel" if a.pm_precision == "fp32" else "pm_kernel",
@@ -299,7 +308,8 @@ def run_ours(a):
                    "evals_per_s": pm_evals / (ms_pm / 1e3),
                    "ms": round(ms_pm, 3), "share_of_step": round(ms_pm / (ms_pm + ms_sweep), 4),
                    "ncu_profile": PM_PROFILE[a.pm_precision],
-                   "issue_active_ncu": 0.583 if a.pm_precision == "fp32" else 0.667,
+                   "issue_active_ncu": ({"propagation": 0.711, "trials": 0.581} if a.pm_precision == "fp32"
+                                        else 0.667),
                    "note": "not a contraction and not HBM-bound (DRAM < 1 %): bound by SIMT issue; "
                            "issue_active is the fraction of SM issue slots used (ncu, see ncu_profile)"}
     L.check_device_faults()        # a sweep tile that gave up its bounded wait makes the run fail
