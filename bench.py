@@ -312,6 +312,29 @@ def run_ours(a):
                                         else 0.667),
                    "note": "not a contraction and not HBM-bound (DRAM < 1 %): bound by SIMT issue; "
                            "issue_active is the fraction of SM issue slots used (ncu, see ncu_profile)"}
+    # the cost of the precision forms of the sweep, each timed once after the timed region on the
+    # same view: compensated FP32 sums (config 3's form; FP16 sources), and the reference's float64
+    # window sums
+    forms = None
+    if world == 1 and a.precision == "fp32":
+        forms = {}
+        s16 = [fast.to_fp16(s) for s in srcs]
+        for name, pv, ss in (("fp16_compensated", L.PREC_FP16_COMP, s16), ("fp64_sums", L.PREC_FP64_SUMS, srcs)):
+            a_f, keep_f = dense.sweep_args(ref, mu, sd, None, ss, geo, ref_cam, hyp, r, top_k, state, precision=pv)
+            ts_f = []
+            for rep in range(2):
+                for t in state[:4]:
+                    t.fill_(-2.0)
+                state[4].fill_(-1)
+                e0f, e1f = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0f.record(stream)
+                L.check(lib.mvs_sweep(ctypes.addressof(a_f), sh), "sweep")
+                e1f.record(stream)
+                e1f.synchronize()
+                if rep:
+                    ts_f.append(e0f.elapsed_time(e1f))
+            forms[name] = {"ms": round(ts_f[0], 3), "vs_fp32": round(ts_f[0] / ms_sweep, 3)}
+        del s16
     L.check_device_faults()        # a sweep tile that gave up its bounded wait makes the run fail
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
     # our kernels per step: the sweep (+ the ordered chunk merge when its planes are split over
@@ -335,6 +358,7 @@ def run_ours(a):
         "roofline_pm": roof_pm,
         "phases_ms": {"sweep": round(ms_sweep, 3), "patchmatch": round(ms_pm, 3)},
         "patchmatch_other_precision": pm_other,
+        "sweep_precision_forms": forms,
         "clocks": clocks.summary(),
         "gpu_launches": launches * a.steps,
         "setup_s": round(setup_s, 1),
