@@ -17,6 +17,7 @@ import numpy as np
 import pytest
 import torch
 
+from conftest import same_bits
 from oracle import oracle as O
 from tests_support import SCORE_ABS, check_parity, gap_of
 
@@ -190,3 +191,39 @@ def test_c3_precision_variant_on_ten_scenes():
     print("C3 depth error vs the float64 oracle (10 scenes, 640x480, 128 planes):", report)
     for name in forms:
         assert report[name]["median"] <= 1e-3, (name, report[name])
+
+
+def test_c2_patchmatch_on_a_crop_of_the_bench_view():
+    """C2's PatchMatch on a 320 x 240 crop of the benchmark's view (8 sources at 4000 x 3000,
+    7 x 7 window, step 1; depth from the device sweep, normals seeded within 30 degrees of
+    vertical): one iteration through the C ABI against the oracle (the reference's pm_refine
+    restated, pinned to it), float64 bit for bit, float32 within 0.1 % on >= 99.9 % of pixels."""
+    from py_ortho_b200 import dense, scene as S
+    sc = S.make_scene("c2", seed=0, device="cuda")
+    srcs = [sc.grey(s) for s in sc.srcs]
+    y0, x0, h, w = 1400, 1800, 240, 320
+    ref = np.ascontiguousarray(sc.grey(sc.ref)[y0:y0 + h, x0:x0 + w])
+    cam = sc.ref_cam
+    # the crop's camera: the same pose, principal point shifted by the crop origin
+    ray = np.ascontiguousarray(O.rays_world((3000, 4000), cam)[:, y0:y0 + h, x0:x0 + w])
+    planes = S.plane_list(60.0, 90.0, 256)
+    st, depth, _, _, _ = _device_sweep(sc.grey(sc.ref), srcs, sc, planes, 3, 2)
+    d0 = np.ascontiguousarray(depth.cpu().numpy()[y0:y0 + h, x0:x0 + w])
+    n0 = S.tilted_normals(h, w, 1000)
+    par = np.array([c.row() for c in sc.src_cams], np.float64)
+    act = np.ones((h, w), np.uint8)
+    args = (3, 1, 2, 0.0, 0.02, 1, 60.0, 90.0, 12345)
+    b = [d0.copy(), n0.copy(), np.zeros((h, w), np.float32)]
+    cb = O.pm_refine(ref, ray, cam.C, srcs, [None] * 8, par, *b, act, *args)
+    for prec in ("fp64", "fp32"):
+        a = [d0.copy(), n0.copy(), np.zeros((h, w), np.float32)]
+        ca = dense.pm_refine(ref, ray, cam.C, srcs, [None] * 8, par, *a, act, *args, precision=prec)
+        if prec == "fp64":
+            assert ca == cb
+            for x, y in zip(a, b):
+                assert same_bits(x, y)
+        else:
+            fin = np.isfinite(b[0])
+            rel = np.abs(a[0][fin].astype(np.float64) - b[0][fin]) / b[0][fin]
+            print(f"C2 crop PatchMatch fp32 vs oracle: within 0.1 % {(rel <= 1e-3).mean():.5f}, median {np.median(rel):.1e}")
+            assert (rel <= 1e-3).mean() >= 0.999
