@@ -278,8 +278,9 @@ typedef struct mvs_pm_args {
  * pass runs propagation for all its pixels in parallel, counts the drawing pixels (a prefix sum
  * in raster order) and jumps the stream to each pixel's offset (GF(2) matrix powers), then runs
  * the trials in parallel. With MVS_PM_FP64 the result is bit-identical to the reference's.
- * Scratch (about 21 bytes per pixel, plus 16 per pixel when iters > 1) is allocated
- * stream-ordered per call. */
+ * Scratch (about 21 bytes per pixel, plus 16 per pixel when iters > 1, plus 16 per source pixel
+ * with MVS_PM_FP32: each source's 2 x 2 bilinear footprints, one 16-byte load per sample) is
+ * allocated stream-ordered per call. */
 mvs_status mvs_pm_refine(const mvs_pm_args* args, void* stream);
 
 /* The xorshift32 state after n steps of the PatchMatch stream from `state` (host; jump-ahead by

@@ -26,6 +26,8 @@
 // call to call), so no step waits for the host.
 #include "common.cuh"
 
+#include <algorithm>
+
 namespace mvs {
 
 struct PMParams {
@@ -52,6 +54,9 @@ struct PMParams {
     int pinhole[MVS_MAX_SOURCES];       // k1 = k2 = k3 = 0
     double par[MVS_MAX_SOURCES * 18];
     double bsrc[MVS_MAX_SOURCES * 3];   // R_s (C_ref - C_s)
+    // float32 lane kernel: per source its 2 x 2 bilinear footprints, quad[y w + x] =
+    // (I(y, x), I(y, x + 1), I(y + 1, x), I(y + 1, x + 1)), one 16-byte load per sample
+    const float4* quad[MVS_MAX_SOURCES];
 };
 
 // ---------------------------------------------------------------- the reference's stream
@@ -497,6 +502,20 @@ __global__ void pm_rng_init_kernel(unsigned* rng, const unsigned* from, unsigned
     rng[0] = from ? *from : seed;
 }
 
+// The 2 x 2 bilinear footprints of a source image (PMParams::quad). The last row and column, which
+// are never a footprint's top-left tap (every tap offset is clamped to (h - 2) w + w - 2), repeat
+// the edge.
+__global__ void __launch_bounds__(256) pm_quad_kernel(const float* __restrict__ im, int w, int h,
+                                                      float4* __restrict__ quad) {
+    const long long n = (long long)w * h;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / w), x = (int)(i - (long long)y * w);
+        const long long r0 = (long long)y * w, r1 = (long long)min(y + 1, h - 1) * w;
+        const int x1 = min(x + 1, w - 1);
+        quad[i] = make_float4(__ldg(im + r0 + x), __ldg(im + r0 + x1), __ldg(im + r1 + x), __ldg(im + r1 + x1));
+    }
+}
+
 // ---------------------------------------------------------------- float32 evaluation (MVS_PM_FP32)
 //
 // The same visits, candidates, draws and acceptance rule as pm_kernel, with the window costs
@@ -537,6 +556,13 @@ __device__ __forceinline__ int pmf_floor(float x, float& f) {   // |x| < 2^22
     return __float_as_int(t) - 0x4B400000;
 }
 
+// The same floor, returning the raw bits of x + 1.5 * 2^23 (floor(x) + 0x4B400000).
+__device__ __forceinline__ unsigned pmf_floor_bits(float x, float& f) {   // |x| < 2^22
+    const float t = __fadd_rd(x, 12582912.0f);
+    f = __fsub_rn(t, 12582912.0f);
+    return (unsigned)__float_as_int(t);
+}
+
 // Window statistics shared by the lanes of a pixel group, fixed for one visit.
 struct PMWin {
     const float4* w;      // NW samples (ray_q - ray_p, I - mI; I = NaN: no sample), then 4 corners
@@ -554,7 +580,8 @@ template <int NSIDE, bool CHECKED, bool ALLFIN>
 __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const float* A, const float* B,
                                                const float* C, float a0, float b0, float c0, float n0, float n1,
                                                float n2, float denp, float lou, float hiu, float lov, float hiv,
-                                               int ub, int vb, const float* im, int sw, int last, float mJ,
+                                               unsigned kb, const float4* qd, int sw, unsigned last,
+                                               float mJ,
                                                float& T1, float& T2, float& X, float& S1, float& S2, float& cnt,
                                                float& ns) {
     // rows rolled, the samples of a row unrolled when the side is known (the checked form, rare,
@@ -581,14 +608,15 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
             vl = ok ? vl : 0.f;
         }
         float fu, fv;
-        const int xi = pmf_floor(ul, fu) + ub + 0x4B400000;
-        const int yi = pmf_floor(vl, fv) + vb + 0x4B400000;
-        // the clamp keeps every tap inside the image whatever the inputs
-        const int o = min(max(yi * sw + xi, 0), last);
-        MVS_BOUND(o >= 0 && o <= last);
+        // top-left tap offset (floor(v) + V0) sw + floor(u) + U0 from the floor bits: one
+        // multiply-add and one add of the unit's constant, wrapping exactly in 32 bits; the clamp
+        // (an offset below 0 wraps above `last`) keeps every tap inside the image whatever the inputs
+        const unsigned xb = pmf_floor_bits(ul, fu), yb = pmf_floor_bits(vl, fv);
+        const unsigned o = min(yb * (unsigned)sw + xb + kb, last);
+        MVS_BOUND(o <= last);
         const float fx = ul - fu, fy = vl - fv;
-        const float* t = im + o;
-        const float t00 = __ldg(t), t01 = __ldg(t + 1), t10 = __ldg(t + sw), t11 = __ldg(t + sw + 1);
+        const float4 q4 = __ldg(qd + o);
+        const float t00 = q4.x, t01 = q4.y, t10 = q4.z, t11 = q4.w;
         const float top = fmaf(fx, t01 - t00, t00), bot = fmaf(fx, t11 - t10, t10);
         const float J = fmaf(fy, bot - top, top);
         if (CHECKED) ok = ok && fabsf(J) <= 3.4e38f;
@@ -657,10 +685,12 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     const int sw = c.iw[sl], sh = c.ih[sl];
     const float lou = (float)(-U0d), lov = (float)(-V0d);
     const float hiu = (float)(((double)sw - 1.001) - U0d), hiv = (float)(((double)sh - 1.001) - V0d);
-    const float* im = c.img[sl];
     // integer tap position = floor bits + (U0 - magic): one add per coordinate
     const int ub = (int)U0d - 0x4B400000, vb = (int)V0d - 0x4B400000;
     const int last = sh * sw - sw - 2;                    // largest valid top-left tap offset
+    // the window sums' tap offset: yb sw + xb + kb for floor bits xb, yb (unsigned, wrapping)
+    const unsigned kb = (unsigned)vb * (unsigned)sw + (unsigned)ub;
+    const float4* qd = c.quad[sl];
     // ---- corners: the whole window in front and inside (outside) the source
     bool den_ok = true, inside = anchor, front_all = true;
     int out_lo_u = 0, out_hi_u = 0, out_lo_v = 0, out_hi_v = 0;
@@ -693,7 +723,8 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
             const int xi = pmf_floor(ul, fu) + ub + 0x4B400000, yi = pmf_floor(vl, fv) + vb + 0x4B400000;
             const int o = min(max(yi * sw + xi, 0), last);
             const float fx = ul - fu, fy = vl - fv;
-            const float t00 = __ldg(im + o), t01 = __ldg(im + o + 1), t10 = __ldg(im + o + sw), t11 = __ldg(im + o + sw + 1);
+            const float4 q4 = __ldg(qd + o);
+            const float t00 = q4.x, t01 = q4.y, t10 = q4.z, t11 = q4.w;
             const float top = fmaf(fx, t01 - t00, t00), bot = fmaf(fx, t11 - t10, t10);
             const float J = fmaf(fy, bot - top, top);
             if (fabsf(J) <= 3.4e38f) mJ = J;
@@ -705,10 +736,10 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     if (!outside && inside) {
         if (wn.allfin) {
             pm_window_sums<NSIDE, false, true>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
-                                               ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+                                               kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
         } else {
             pm_window_sums<NSIDE, false, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
-                                                ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+                                                kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
         }
         // a non-finite source value in the window poisons the sums: redo the source checked
         if (fabsf(T2) <= 3.4e38f && fabsf(X) <= 3.4e38f) {
@@ -722,7 +753,7 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     if (checked) {
         T1 = T2 = X = S1 = S2 = cnt = ns = 0.f;
         pm_window_sums<NSIDE, true, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
-                                           ub, vb, im, sw, last, mJ, T1, T2, X, S1, S2, cnt, ns);
+                                           kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
     }
     // samples counted by the reference (finite reference value, n.ray_q < -1e-9): with every
     // corner's n.ray_q < -1e-3 that is every finite sample; otherwise each lane counted them
@@ -1136,7 +1167,11 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
     auto up = [](size_t v) { return (v + 255) & ~(size_t)255; };
     const size_t o_best = 0, o_sc = o_best + up(n * 8), o_state = o_sc + up(n * 8), o_flags = o_state + up(n * 4);
     const size_t o_bsum = o_flags + up(n), o_rng = o_bsum + up((size_t)nb * 4), o_cache = o_rng + 256;
-    const size_t bytes = o_cache + (use_cache ? (size_t)HW * 2 * sizeof(double) : 0);
+    const size_t o_quad = o_cache + up(use_cache ? (size_t)HW * 2 * sizeof(double) : 0);
+    size_t quad_bytes = 0;
+    if (fast)
+        for (int s = 0; s < a->S; ++s) quad_bytes += up((size_t)a->src_w[s] * a->src_h[s] * sizeof(float4));
+    const size_t bytes = o_quad + quad_bytes;
     char* scratch = nullptr;
     MVS_CUDA(cudaMallocAsync((void**)&scratch, bytes, st), "pm_refine: scratch");
     p.pbest = reinterpret_cast<double*>(scratch + o_best);
@@ -1150,6 +1185,17 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         p.cost_cache = reinterpret_cast<double*>(scratch + o_cache);
         p.score_cache = p.cost_cache + HW;
         cudaMemsetAsync(p.cost_cache, 0xFF, (size_t)HW * sizeof(double), st);   // all-ones = NaN: recompute
+    }
+    if (fast) {
+        size_t off = o_quad;
+        for (int s = 0; s < a->S; ++s) {
+            float4* q = reinterpret_cast<float4*>(scratch + off);
+            p.quad[s] = q;
+            off += up((size_t)a->src_w[s] * a->src_h[s] * sizeof(float4));
+            const long long ns = (long long)a->src_w[s] * a->src_h[s];
+            const int qb = (int)std::min<long long>((ns + 255) / 256, 148LL * 8);
+            pm_quad_kernel<<<qb, 256, 0, st>>>(a->src[s], a->src_w[s], a->src_h[s], q);
+        }
     }
     const PMJump& J = stream_tables().J;
     // float32 lanes: one per source; a block holds as many pixel groups as its staged windows fit

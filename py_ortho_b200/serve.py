@@ -97,6 +97,9 @@ def footprint(req: DepthRequest, shared_sources: bool = False) -> int:
         b += sum(int(np.prod(s.shape)) * 4 for s in req.srcs)
     if req.pm_iters:
         b += px * 4 * (3 + 3 + 1) + px            # ray, normal, score, active
+        # mvs_pm_refine's scratch while a step runs it: per-pixel pass state and cost cache, and
+        # the float32 mode's 2 x 2 footprints of every source
+        b += px * (21 + 16) + sum(int(np.prod(s.shape)) * 16 for s in req.srcs)
     return b
 
 

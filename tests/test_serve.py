@@ -24,5 +24,6 @@ def test_footprint_counts_resident_buffers():
     assert footprint(req, shared_sources=True) == base
     assert footprint(req) == base + 4 * H * W * 4
     req.pm_iters = 4
-    assert footprint(req, shared_sources=True) == base + H * W * (4 * 7 + 1)
+    # + ray, normal, score, active; + PatchMatch scratch (pass state, cost cache, the sources' footprints)
+    assert footprint(req, shared_sources=True) == base + H * W * (4 * 7 + 1) + H * W * 37 + 4 * H * W * 16
     assert req.evals == H * W * 96 * 4 + H * W * 4 * 11 * 4
