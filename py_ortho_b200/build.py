@@ -6,6 +6,7 @@ Usage: ``python -m py_ortho_b200.build [--force] [--verbose]``. Objects go to
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -54,6 +55,7 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, 
     headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cuh")]
     headers.append(os.path.join(INCLUDE, "mvs_b200.h"))
     objs = []
+    jobs = []
     cc = nvcc()
     for src in SOURCES:
         path = os.path.join(CSRC, src)
@@ -67,11 +69,15 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False, 
                 cmd += ["-Xptxas", "-v"]
             if verbose:
                 print(" ".join(cmd), flush=True)
-            r = subprocess.run(cmd, capture_output=True, text=True)
-            if r.returncode != 0:
-                raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
-            if ptxas_info or verbose:
-                sys.stdout.write(r.stdout + r.stderr)
+            jobs.append((src, cmd))
+    # the translation units compile in parallel (one nvcc per source file)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(lambda j: (j[0], subprocess.run(j[1], capture_output=True, text=True)), jobs))
+    for src, r in results:
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{r.stdout}\n{r.stderr}")
+        if ptxas_info or verbose:
+            sys.stdout.write(r.stdout + r.stderr)
     if force or _stale(lib, objs):
         tmp = lib + ".partial"              # linked aside, then moved into place in one step
         cmd = [cc, "-shared", "-o", tmp] + objs + ARCH + ["-Xcompiler", "-fPIC"]
