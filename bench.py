@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (jobs/s)")
     ap.add_argument("--serve-precision", choices=["fp32", "fp16"], default="fp16")
+    ap.add_argument("--tile-h", type=int, choices=[0, 16, 32, 64], default=0,
+                    help="rows of the sweep's 64-column output tiles (0 = 32)")
     ap.add_argument("--no-modes", action="store_true",
                     help="headline only: skip the batched (config 4) and served (config 5) summaries that a "
                          "1-GPU run appends to its line")
@@ -180,7 +182,8 @@ def run_ours(a):
     lib = L.load()
     stream = torch.cuda.current_stream()
     sh = L.stream_handle()
-    a_sw, keep = dense.sweep_args(ref, mu, sd, None, srcs_k, geo, ref_cam, hyp, r, top_k, state, precision=prec)
+    a_sw, keep = dense.sweep_args(ref, mu, sd, None, srcs_k, geo, ref_cam, hyp, r, top_k, state, precision=prec,
+                                  tile_h=a.tile_h)
     pm = L.PMArgs()
     pm.H, pm.W, pm.S = H, W, nsrc
     pm.ref, pm.ray, pm.Cr = ref.data_ptr(), ray.data_ptr(), L.host_ptr(Cr)
@@ -335,14 +338,40 @@ def run_ours(a):
                     ts_f.append(e0f.elapsed_time(e1f))
             forms[name] = {"ms": round(ts_f[0], 3), "vs_fp32": round(ts_f[0] / ms_sweep, 3)}
         del s16
+    # the same sweep at the other tile shapes (64 x 16 on 128 threads, 64 x 64 on 512), timed once
+    # each after the timed region
+    shapes = None
+    if world == 1 and prec in (L.PREC_FP32, L.PREC_FP16) and top_k <= 2:
+        shapes = {f"64x{a.tile_h or 32}": round(ms_sweep, 3)}
+        for th in (16, 32, 64):
+            if th == (a.tile_h or 32):
+                continue
+            a_t, keep_t = dense.sweep_args(ref, mu, sd, None, srcs_k, geo, ref_cam, hyp, r, top_k, state,
+                                           precision=prec, tile_h=th)
+            ts_t = []
+            for rep in range(2):
+                for t in state[:4]:
+                    t.fill_(-2.0)
+                state[4].fill_(-1)
+                e0t, e1t = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0t.record(stream)
+                L.check(lib.mvs_sweep(ctypes.addressof(a_t), sh), "sweep")
+                e1t.record(stream)
+                e1t.synchronize()
+                if rep:
+                    ts_t.append(e0t.elapsed_time(e1t))
+            shapes[f"64x{th}"] = round(ts_t[0], 3)
     L.check_device_faults()        # a sweep tile that gave up its bounded wait makes the run fail
     dominant = "pm" if ms_pm > ms_sweep else "sweep"
     # our kernels per step: the sweep (+ the ordered chunk merge when its planes are split over
     # CTAs: mvs_sweep's automatic rule, tiles below 6 CTAs per SM), finalize, and per PatchMatch
-    # call the stream start plus, per colour pass, propagation, count, scan, stream states, trials
-    tiles = ((W + 63) // 64) * ((H + 31) // 32)
+    # call the stream start, the float32 mode's footprint images (one launch per source) and, per
+    # colour pass, propagation, count, scan, stream states, trials
+    th_ = a.tile_h or 32
+    tiles = ((W + 63) // 64) * ((H + th_ - 1) // th_)
     sweep_launches = 1 if tiles >= 6 * torch.cuda.get_device_properties(dev).multi_processor_count else 2
-    launches = sweep_launches + 1 + ((1 + 10 * iters) if iters else 0)
+    fp_launches = nsrc if a.pm_precision == "fp32" else 0
+    launches = sweep_launches + 1 + ((1 + fp_launches + 10 * iters) if iters else 0)
     line = {
         "metric": "ZNCC evaluations/s (pixel x plane x view), sweep + PatchMatch",
         "value": value / 1e9, "unit": "Gpix.plane.view/s", "n_gpus": world, "steps": a.steps,
@@ -359,6 +388,7 @@ def run_ours(a):
         "phases_ms": {"sweep": round(ms_sweep, 3), "patchmatch": round(ms_pm, 3)},
         "patchmatch_other_precision": pm_other,
         "sweep_precision_forms": forms,
+        "sweep_tile_heights_ms": shapes,
         "clocks": clocks.summary(),
         "gpu_launches": launches * a.steps,
         "setup_s": round(setup_s, 1),
@@ -680,7 +710,7 @@ def run_batch(a):
 
 def batch_summary(a, dev):
     """Config 4: per-view launches (plain single-view kernel) vs one persistent batched launch in
-    a CUDA graph (autotuned plane chunk / CTAs per SM), FP32 and FP16 storage."""
+    a CUDA graph (autotuned plane chunk and tile height), FP32 and FP16 storage."""
     import torch
     from py_ortho_b200 import _lib as L, batch, dense, fast
     t0 = time.time()
@@ -705,11 +735,11 @@ def batch_summary(a, dev):
           for j in jobs]
     torch.cuda.synchronize()
 
-    def plain():
+    def plain(tile_h=0):
         for v in vj:
             hyp = dense.Hypotheses.planes_inv(v.planes_inv)
             stt = dense.sweep(v.ref, v.mu, v.sd, None, v.srcs, batch._geo(v.ref_cam, v.src_cams), hyp, v.r, v.top_k,
-                              state=v.state, ref_cam=fast.cam_row(v.ref_cam))
+                              state=v.state, ref_cam=fast.cam_row(v.ref_cam), tile_h=tile_h)
             dense.finalize(hyp, stt, out=v.depth)
             for t in v.state[:4]:
                 t.fill_(-2.0)
@@ -717,10 +747,24 @@ def batch_summary(a, dev):
 
     ms_plain = timed(plain)
     d_plain = [v.depth.clone() for v in vj]
-    best, table = batch.autotune(vj, chunks=(0, 128), ctas=(0, 1), reps=1)
+    # the autotuner's search: plane chunk x tile height (one CTA count: the occupancy maximum, which
+    # every earlier search picked)
+    best, table = batch.autotune(vj, chunks=(0, 128), ctas=(0,), tile_hs=(16, 32, 64), reps=1)
     ms_batch = timed(lambda: best.run(graph=True), reps=2)
-    same = all(torch.equal(v.depth, d) for v, d in zip(vj, d_plain))
+    d_batch = [v.depth.clone() for v in vj]
+    th = best.tile_h
     best.close()
+    d_same_tile = d_plain
+    if th != 32:   # the plain kernel at the tuned tile height (bit-identity holds per tile shape)
+        plain(th)
+        torch.cuda.synchronize()
+        d_same_tile = [v.depth.clone() for v in vj]
+    same = all(torch.equal(x, d) for x, d in zip(d_batch, d_same_tile))
+    rel_th = []
+    for x, d in zip(d_batch, d_plain):
+        m = torch.isfinite(x) & torch.isfinite(d) & (d > 0)
+        rel_th.append(((x.double() - d.double()).abs() / d.double())[m].cpu().numpy())
+    rel_th = np.concatenate(rel_th)
     # FP16 storage of the (shared) sources
     h16 = {}
     vj16 = []
@@ -732,10 +776,10 @@ def batch_summary(a, dev):
                 h16[key] = fast.to_fp16(s_)
             srcs16.append(h16[key])
         vj16.append(batch.ViewJob(v.ref, srcs16, v.ref_cam, v.src_cams, v.planes_inv, r=v.r, top_k=2).prepare())
-    best16, table16 = batch.autotune(vj16, precision=L.PREC_FP16, chunks=(0, 128), ctas=(0, 1), reps=1)
+    best16, table16 = batch.autotune(vj16, precision=L.PREC_FP16, chunks=(0, 128), ctas=(0,), tile_hs=(th,), reps=1)
     ms_16 = timed(lambda: best16.run(graph=True), reps=2)
     rel = []
-    for v16, d in zip(vj16, d_plain):
+    for v16, d in zip(vj16, d_same_tile):
         x, y = v16.depth.double(), d.double()
         m = torch.isfinite(x) & torch.isfinite(y) & (y > 0)
         rel.append(((x - y).abs() / y)[m].cpu().numpy())
@@ -745,12 +789,14 @@ def batch_summary(a, dev):
             "jobs": len(jobs), "evals": evals, "setup_s": round(setup, 1),
             "plain_per_view": {"ms": round(ms_plain, 2), "value": evals / (ms_plain / 1e3) / 1e9},
             "batched_fp32": {"ms": round(ms_batch, 2), "value": evals / (ms_batch / 1e3) / 1e9,
-                             "identical_to_plain": bool(same), "autotune_ms": [(c, k, round(t, 2)) for c, k, t in table],
-                             "work_items": None},
+                             "tile": f"64x{th}", "identical_to_plain_same_tile": bool(same),
+                             "depth_rel_vs_plain_64x32": {"median": float(np.median(rel_th)),
+                                                          "within_0.1pct": float((rel_th <= 1e-3).mean())},
+                             "autotune_ms": [(c, k, t_h, round(t, 2)) for c, k, t_h, t in table]},
             "batched_fp16": {"ms": round(ms_16, 2), "value": evals / (ms_16 / 1e3) / 1e9,
                              "depth_rel_err_vs_fp32_median": float(np.median(rel)),
                              "depth_rel_err_vs_fp32_p99": float(np.percentile(rel, 99)),
-                             "autotune_ms": [(c, k, round(t, 2)) for c, k, t in table16]},
+                             "autotune_ms": [(c, k, t_h, round(t, 2)) for c, k, t_h, t in table16]},
             "speedup_fp16_batched_vs_plain": ms_plain / ms_16, "speedup_fp32_batched_vs_plain": ms_plain / ms_batch,
             "config": {"workload": "c4: 64 views, long side U(1200,4000) 4:3, 4-12 sources, 96-384 planes, 5x5/7x7",
                        "flight": "4x4 grid, 75 % overlap, 4000x3000, f=3600, 80 m; references are crops"}}

@@ -103,7 +103,9 @@ typedef struct mvs_sweep_args {
     int32_t r;                             /* window radius, 0 .. MVS_MAX_RADIUS                */
     int32_t top_k;                         /* score = mean of the best top_k source NCCs        */
     int32_t plane_chunks;                  /* 0 = automatic; else CTAs per tile along planes   */
-    int32_t pad_;
+    int32_t tile_h;                        /* output tile rows: 0 (= 32), 16, 32 or 64; tiles are
+                                              64 columns wide. 16 and 64: FP32 / FP16 PLANES
+                                              sweeps with top_k <= 2 (other forms: 0 or 32)      */
     float* best;                           /* (H, W) in/out winner-take-all state               */
     float* prev;
     float* s_prev_best;
@@ -297,6 +299,9 @@ typedef struct mvs_batch_job {
 typedef struct mvs_batch_tuning {
     int32_t plane_chunk;                   /* planes per work item (0 = autotuned)             */
     int32_t ctas_per_sm;                   /* persistent CTAs per SM (0 = occupancy maximum)  */
+    int32_t tile_h;                        /* rows of the plan's 64-column output tiles: 0 (= 32),
+                                              16, 32 or 64 (16 and 64: top_k <= 2 in every job);
+                                              the jobs' own mvs_sweep_args.tile_h is not read    */
 } mvs_batch_tuning;
 
 typedef struct mvs_batch mvs_batch;        /* opaque: device work list, job table, graph       */

@@ -45,7 +45,7 @@ class SweepArgs(C.Structure):
                 ("n_src", i32), ("precision", i32), ("src", vp * MAX_SOURCES),
                 ("src_h", i32 * MAX_SOURCES), ("src_w", i32 * MAX_SOURCES), ("geo", vp), ("ref_cam", vp),
                 ("hyp", Hyp), ("i0", i32), ("i1", i32), ("r", i32), ("top_k", i32), ("plane_chunks", i32),
-                ("pad_", i32), ("best", vp), ("prev", vp), ("s_prev_best", vp), ("s_next_best", vp),
+                ("tile_h", i32), ("best", vp), ("prev", vp), ("s_prev_best", vp), ("s_next_best", vp),
                 ("idx", vp)]
 
 
@@ -97,7 +97,7 @@ class BatchJob(C.Structure):
 
 
 class BatchTuning(C.Structure):
-    _fields_ = [("plane_chunk", i32), ("ctas_per_sm", i32)]
+    _fields_ = [("plane_chunk", i32), ("ctas_per_sm", i32), ("tile_h", i32)]
 
 
 # name -> (restype, argtypes); every symbol the header declares

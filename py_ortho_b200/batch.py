@@ -1,6 +1,6 @@
 """Batched depth maps: many reference views of uneven size, source count, plane count and window
 radius in one persistent launch (mvs_batch_*), replayed as a CUDA graph, with a small
-autotuner for the plane-chunk size and CTAs per SM.
+autotuner for the plane-chunk size, CTAs per SM and tile height.
 
 A job is one view swept over constant inverse-depth planes (pinhole cameras). Its result does
 not depend on the other jobs of the batch (per-pixel reduction order is fixed by plane index).
@@ -64,9 +64,11 @@ def _geo(ref_cam, src_cams):
 class Batch:
     """A persistent batched plan (mvs_batch_create); run() replays it (CUDA graph by default)."""
 
-    def __init__(self, jobs, plane_chunk: int = 0, ctas_per_sm: int = 0, precision: int = L.PREC_FP32):
+    def __init__(self, jobs, plane_chunk: int = 0, ctas_per_sm: int = 0, precision: int = L.PREC_FP32,
+                 tile_h: int = 0):
         self.jobs = jobs
         self.precision = precision
+        self.tile_h = int(tile_h) or 32
         arr = (L.BatchJob * len(jobs))()
         self._keep = []
         for j, job in enumerate(jobs):
@@ -78,7 +80,7 @@ class Batch:
             arr[j].sweep = a
             arr[j].depth = job.depth.data_ptr()
             self._keep.append(keep)
-        tun = L.BatchTuning(int(plane_chunk), int(ctas_per_sm))
+        tun = L.BatchTuning(int(plane_chunk), int(ctas_per_sm), int(tile_h))
         h = ctypes.c_void_p()
         L.check(L.load().mvs_batch_create(ctypes.addressof(arr), len(jobs), ctypes.addressof(tun), ctypes.byref(h)),
                 "batch_create")
@@ -118,26 +120,29 @@ def time_plan(b: Batch, reps: int = 3, stream=None) -> float:
 _TUNE_CACHE: dict = {}
 
 
-def autotune(jobs, precision: int = L.PREC_FP32, chunks=(0, 16, 32, 64), ctas=(0, 1), reps: int = 2):
-    """Picks (plane_chunk, ctas_per_sm) by timing each candidate plan on the actual jobs; results
-    are cached per job-shape signature. Returns (best_batch, table of (chunk, ctas, ms))."""
-    key = (precision, tuple((int(j.ref.shape[0]), int(j.ref.shape[1]), len(j.srcs), len(j.planes_inv), j.r)
-                            for j in jobs))
+def autotune(jobs, precision: int = L.PREC_FP32, chunks=(0, 16, 32, 64), ctas=(0, 1), tile_hs=(32,), reps: int = 2):
+    """Picks (plane_chunk, ctas_per_sm, tile_h) by timing each candidate plan on the actual jobs
+    (tile_h: rows of the 64-column output tiles, 16 / 32 / 64; 16 and 64 need top_k <= 2);
+    results are cached per job-shape signature. Returns (best_batch, table of
+    (chunk, ctas, tile_h, ms))."""
+    key = (precision, tuple(tile_hs), tuple((int(j.ref.shape[0]), int(j.ref.shape[1]), len(j.srcs),
+                                             len(j.planes_inv), j.r, j.top_k) for j in jobs))
     table = []
     if key in _TUNE_CACHE:
-        pc, cps = _TUNE_CACHE[key]
-        return Batch(jobs, pc, cps, precision), table
+        pc, cps, th = _TUNE_CACHE[key]
+        return Batch(jobs, pc, cps, precision, th), table
     best = None
-    for pc in chunks:
-        for cps in ctas:
-            b = Batch(jobs, pc, cps, precision)
-            ms = time_plan(b, reps)
-            table.append((pc, cps, ms))
-            if best is None or ms < best[0]:
-                if best is not None:
-                    best[1].close()
-                best = (ms, b, pc, cps)
-            else:
-                b.close()
-    _TUNE_CACHE[key] = (best[2], best[3])
+    for th in tile_hs:
+        for pc in chunks:
+            for cps in ctas:
+                b = Batch(jobs, pc, cps, precision, th)
+                ms = time_plan(b, reps)
+                table.append((pc, cps, th, ms))
+                if best is None or ms < best[0]:
+                    if best is not None:
+                        best[1].close()
+                    best = (ms, b, pc, cps, th)
+                else:
+                    b.close()
+    _TUNE_CACHE[key] = (best[2], best[3], best[4])
     return best[1], table

@@ -32,14 +32,15 @@ struct JobFin {                        // per-job table of the merge / finalize 
 // One radius of the tile engine as an out-of-line call: the persistent kernel dispatches on the
 // work item's radius, and keeping each instance out of line gives each its own register
 // allocation (inlined together, the largest instance's pressure spilled the others).
-template <int R, int KMAX, bool F16, bool WIDE>
+template <int R, int KMAX, bool F16, bool WIDE, int TH>
 __device__ __noinline__ void batch_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int ch, float* smem) {
-    sweep_tile<R, KMAX, true, F16, WIDE>(p, tx, ty, pa, pb, ch, smem);
+    sweep_tile<R, KMAX, true, F16, WIDE, false, false, false, TH>(p, tx, ty, pa, pb, ch, smem);
 }
 
-template <int RMAX, int KMAX, bool F16>
-__global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restrict__ jobs, const int4* __restrict__ items,
-                                                      int n_items, int* counter) {
+// TH: the plan's tile height (one shape per persistent launch; 64 x TH tiles on 8 TH threads)
+template <int RMAX, int KMAX, bool F16, int TH = TH_DEFAULT>
+__global__ void __launch_bounds__(TileShape<TH>::NT, TileShape<TH>::MIN_CTAS)
+    batch_kernel(const SweepParams* __restrict__ jobs, const int4* __restrict__ items, int n_items, int* counter) {
     extern __shared__ float4 smem4[];
     __shared__ int s_item;
     float* smem = reinterpret_cast<float*>(smem4);
@@ -58,17 +59,17 @@ __global__ void __launch_bounds__(NT, 2) batch_kernel(const SweepParams* __restr
         const int tx = w.y * TW, ty = w.z * TH;
         // the radius is uniform per work item: each case is the single-view instance itself
         switch (p.r) {
-            case 0: batch_tile<0, KMAX, F16, false>(p, tx, ty, pa, pb, ch, smem); break;
-            case 1: batch_tile<1, KMAX, F16, false>(p, tx, ty, pa, pb, ch, smem); break;
-            case 2: batch_tile<2, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
-            case 3: batch_tile<3, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+            case 0: batch_tile<0, KMAX, F16, false, TH>(p, tx, ty, pa, pb, ch, smem); break;
+            case 1: batch_tile<1, KMAX, F16, false, TH>(p, tx, ty, pa, pb, ch, smem); break;
+            case 2: batch_tile<2, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
+            case 3: batch_tile<3, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
             default:
                 if constexpr (RMAX > 3) {
                     switch (p.r) {
-                        case 4: batch_tile<4, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
-                        case 5: batch_tile<5, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
-                        case 6: batch_tile<6, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
-                        default: batch_tile<7, KMAX, F16, true>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 4: batch_tile<4, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 5: batch_tile<5, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
+                        case 6: batch_tile<6, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
+                        default: batch_tile<7, KMAX, F16, true, TH>(p, tx, ty, pa, pb, ch, smem); break;
                     }
                 }
         }
@@ -102,18 +103,57 @@ __global__ void batch_finalize_kernel(const JobFin* __restrict__ jobs, int n_job
     if (j.depth) j.depth[o] = finalize_pixel(j.p0, j.p1, j.n, B, SP, SN, I);
 }
 
-template <int RMAX, int KMAX, bool F16>
+template <int RMAX, int KMAX, bool F16, int TH = TH_DEFAULT>
 static mvs_status batch_attr(int* max_ctas_per_sm) {
-    auto kern = batch_kernel<RMAX, KMAX, F16>;
-    const size_t smem = smem_bytes_upto<RMAX>();
+    auto kern = batch_kernel<RMAX, KMAX, F16, TH>;
+    const size_t smem = smem_bytes_upto<RMAX, TH>();
     MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "batch: smem attribute");
-    MVS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_ctas_per_sm, kern, NT, smem), "batch: occupancy");
+    MVS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(max_ctas_per_sm, kern, TileShape<TH>::NT, smem),
+             "batch: occupancy");
     return MVS_OK;
 }
 
-template <int RMAX, int KMAX, bool F16>
+template <int RMAX, int KMAX, bool F16, int TH = TH_DEFAULT>
 static void batch_launch(dim3 grid, cudaStream_t st, const SweepParams* jobs, const int4* items, int n, int* counter) {
-    batch_kernel<RMAX, KMAX, F16><<<grid, NT, smem_bytes_upto<RMAX>(), st>>>(jobs, items, n, counter);
+    batch_kernel<RMAX, KMAX, F16, TH><<<grid, TileShape<TH>::NT, smem_bytes_upto<RMAX, TH>(), st>>>(jobs, items, n,
+                                                                                                 counter);
+}
+
+// The plan's kernel for radius class RMAX (3 or 7), list size KMAX (2 or 8), storage and tile
+// height: attribute query (Q) or launch. Tile heights 16 and 64 exist for 2-entry lists only.
+template <int RMAX, int KMAX, bool F16>
+static mvs_status batch_select(int th, bool query, int* cps, dim3 grid, cudaStream_t st, const SweepParams* jobs,
+                               const int4* items, int n, int* counter) {
+    if constexpr (KMAX == 2) {
+        if (th == 16) {
+            if (query) return batch_attr<RMAX, 2, F16, 16>(cps);
+            batch_launch<RMAX, 2, F16, 16>(grid, st, jobs, items, n, counter);
+            return MVS_OK;
+        }
+        if (th == 64) {
+            if (query) return batch_attr<RMAX, 2, F16, 64>(cps);
+            batch_launch<RMAX, 2, F16, 64>(grid, st, jobs, items, n, counter);
+            return MVS_OK;
+        }
+    }
+    if (th != TH_DEFAULT) return fail(MVS_ERR_UNSUPPORTED, "batch: tile height %d needs top_k <= 2", th);
+    if (query) return batch_attr<RMAX, KMAX, F16>(cps);
+    batch_launch<RMAX, KMAX, F16>(grid, st, jobs, items, n, counter);
+    return MVS_OK;
+}
+
+static mvs_status batch_kernel_for(int rmax, int kmax, bool f16, int th, bool query, int* cps, dim3 grid,
+                                   cudaStream_t st, const SweepParams* jobs, const int4* items, int n, int* counter) {
+    if (rmax <= 3) {
+        if (kmax <= 2) return f16 ? batch_select<3, 2, true>(th, query, cps, grid, st, jobs, items, n, counter)
+                                  : batch_select<3, 2, false>(th, query, cps, grid, st, jobs, items, n, counter);
+        return f16 ? batch_select<3, 8, true>(th, query, cps, grid, st, jobs, items, n, counter)
+                   : batch_select<3, 8, false>(th, query, cps, grid, st, jobs, items, n, counter);
+    }
+    if (kmax <= 2) return f16 ? batch_select<7, 2, true>(th, query, cps, grid, st, jobs, items, n, counter)
+                              : batch_select<7, 2, false>(th, query, cps, grid, st, jobs, items, n, counter);
+    return f16 ? batch_select<7, 8, true>(th, query, cps, grid, st, jobs, items, n, counter)
+               : batch_select<7, 8, false>(th, query, cps, grid, st, jobs, items, n, counter);
 }
 
 }  // namespace mvs
@@ -124,6 +164,7 @@ struct mvs_batch {
     int n_jobs = 0;
     int rmax = 3, kmax = 2;
     bool f16 = false;
+    int th = TH_DEFAULT;               // tile height of the plan
     int grid = 0;
     int n_items = 0;
     long long evals = 0;
@@ -141,23 +182,8 @@ struct mvs_batch {
 static mvs_status batch_enqueue(mvs_batch* b, cudaStream_t st) {
     MVS_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(int), st), "batch: reset counter");
     const dim3 grid(b->grid);
-    if (b->rmax <= 3) {
-        if (b->kmax <= 2) {
-            if (b->f16) batch_launch<3, 2, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-            else batch_launch<3, 2, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-        } else {
-            if (b->f16) batch_launch<3, 8, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-            else batch_launch<3, 8, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-        }
-    } else {
-        if (b->kmax <= 2) {
-            if (b->f16) batch_launch<7, 2, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-            else batch_launch<7, 2, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-        } else {
-            if (b->f16) batch_launch<7, 8, true>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-            else batch_launch<7, 8, false>(grid, st, b->d_params, b->d_items, b->n_items, b->d_counter);
-        }
-    }
+    MVS_TRY(batch_kernel_for(b->rmax, b->kmax, b->f16, b->th, false, nullptr, grid, st, b->d_params, b->d_items,
+                             b->n_items, b->d_counter));
     MVS_TRY(check_launch("batch persistent kernel"));
     batch_finalize_kernel<<<(unsigned)b->fin_blocks, 256, 0, st>>>(b->d_fin, b->n_jobs);
     return check_launch("batch finalize kernel");
@@ -184,7 +210,9 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
     if (!jobs || n_jobs < 1) return fail(MVS_ERR_VALUE, "batch: needs at least one job");
     const int pc_req = tuning ? tuning->plane_chunk : 0;
     const int cps_req = tuning ? tuning->ctas_per_sm : 0;
+    const int th = tuning && tuning->tile_h ? tuning->tile_h : TH_DEFAULT;
     if (pc_req < 0 || cps_req < 0) return fail(MVS_ERR_VALUE, "batch: negative tuning value");
+    if (th != 16 && th != 32 && th != 64) return fail(MVS_ERR_VALUE, "batch: tile height %d is not 0, 16, 32 or 64", th);
     std::vector<SweepParams> params(n_jobs);
     std::vector<JobFin> fin(n_jobs);
     std::vector<int4> items;
@@ -192,11 +220,15 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
     long long rec_floats = 0;
     mvs_batch* b = new mvs_batch();
     b->n_jobs = n_jobs;
+    b->th = th;
     b->f16 = jobs[0].sweep.precision == MVS_PREC_FP16;
     int rmax = 0, kmax = 2;
     std::vector<long long> rec_off(n_jobs, -1);
     for (int j = 0; j < n_jobs; ++j) {
-        const mvs_sweep_args* a = &jobs[j].sweep;
+        // the plan's tile height applies to every job (the jobs' own tile_h is not read)
+        mvs_sweep_args ja = jobs[j].sweep;
+        ja.tile_h = 0;
+        const mvs_sweep_args* a = &ja;
         mvs_status st = validate_sweep(a);
         if (st != MVS_OK) { batch_free(b); return st; }
         if (a->hyp.kind != MVS_HYP_PLANES) { batch_free(b); return fail(MVS_ERR_VALUE, "batch: job %d must use MVS_HYP_PLANES", j); }
@@ -221,7 +253,7 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
         const int pc = pc_req > 0 ? std::min(pc_req, n) : n;
         p.ppc = pc;
         p.nchunks = (n + pc - 1) / pc;
-        const int tx = (a->W + TW - 1) / TW, ty = (a->H + TH - 1) / TH;
+        const int tx = (a->W + TW - 1) / TW, ty = (a->H + th - 1) / th;
         if (p.nchunks > 1) {
             rec_off[j] = rec_floats;
             rec_floats += (long long)6 * p.nchunks * a->H * a->W;
@@ -231,7 +263,7 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
             for (int y = 0; y < ty; ++y)
                 for (int x = 0; x < tx; ++x) {
                     items.push_back(make_int4(j, x, y, ch));
-                    cost.push_back((long long)planes * a->n_src * (TW + 2 * a->r) * (TH + 2 * a->r));
+                    cost.push_back((long long)planes * a->n_src * (TW + 2 * a->r) * (th + 2 * a->r));
                 }
         }
         b->evals += (long long)a->H * a->W * n * a->n_src;
@@ -245,6 +277,10 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
     }
     b->rmax = rmax <= 3 ? 3 : 7;
     b->kmax = kmax;
+    if (th != TH_DEFAULT && kmax > 2) {
+        batch_free(b);
+        return fail(MVS_ERR_UNSUPPORTED, "batch: tile height %d needs top_k <= 2 in every job", th);
+    }
     // largest items first
     std::vector<int> order(items.size());
     for (size_t i = 0; i < order.size(); ++i) order[i] = (int)i;
@@ -254,11 +290,8 @@ extern "C" mvs_status mvs_batch_create(const mvs_batch_job* jobs, int32_t n_jobs
     b->n_items = (int)sorted.size();
 
     int max_cps = 0;
-    mvs_status st = MVS_OK;
-    if (b->rmax <= 3) st = b->kmax <= 2 ? (b->f16 ? batch_attr<3, 2, true>(&max_cps) : batch_attr<3, 2, false>(&max_cps))
-                                        : (b->f16 ? batch_attr<3, 8, true>(&max_cps) : batch_attr<3, 8, false>(&max_cps));
-    else st = b->kmax <= 2 ? (b->f16 ? batch_attr<7, 2, true>(&max_cps) : batch_attr<7, 2, false>(&max_cps))
-                           : (b->f16 ? batch_attr<7, 8, true>(&max_cps) : batch_attr<7, 8, false>(&max_cps));
+    mvs_status st = batch_kernel_for(b->rmax, b->kmax, b->f16, th, true, &max_cps, dim3(1), nullptr, nullptr, nullptr,
+                                     0, nullptr);
     if (st != MVS_OK) { batch_free(b); return st; }
     if (max_cps < 1) { batch_free(b); return fail(MVS_ERR_CUDA, "batch: kernel does not fit on an SM"); }
     const int cps = cps_req > 0 ? std::min(cps_req, max_cps) : max_cps;
@@ -478,7 +511,7 @@ extern "C" mvs_status mvs_server_step(mvs_server* s, const int32_t* slots, const
         const SweepParams& p = s->h_params[sl];
         const int pa = p.i0 + chunks[k] * p.ppc;
         if (chunks[k] < 0 || pa >= p.i1) return fail(MVS_ERR_VALUE, "server: chunk %d beyond job %d", chunks[k], sl);
-        const int tx = (p.W + TW - 1) / TW, ty = (p.H + TH - 1) / TH;
+        const int tx = (p.W + TW - 1) / TW, ty = (p.H + TH_DEFAULT - 1) / TH_DEFAULT;
         if (items + tx * ty > s->max_items) return fail(MVS_ERR_VALUE, "server: step exceeds %d work items", s->max_items);
         for (int y = 0; y < ty; ++y)
             for (int x = 0; x < tx; ++x) s->h_items[items++] = make_int4(sl, x, y, chunks[k]);

@@ -25,16 +25,16 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return fn;
 }
 
-// The reference's 2D tiled map for the tile copy: box = the tile with its halo (Geom<r>::JP x
-// Geom<r>::HR floats). Needs a 16-byte aligned base and a row pitch that is a multiple of 16
+// The reference's 2D tiled map for the tile copy: box = the tile with its halo (Geom<r, th>::JP x
+// Geom<r, th>::HR floats). Needs a 16-byte aligned base and a row pitch that is a multiple of 16
 // bytes (W % 4 == 0); otherwise the tile is loaded by the threads (same values).
-static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r) {
+static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r, int th) {
     PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
     if (!enc || !ref || (reinterpret_cast<uintptr_t>(ref) & 15u) || W % 4 != 0 || W < 1 || H < 1) return false;
     const int RA = (r + 3) & ~3;
     const cuuint64_t dims[2] = {(cuuint64_t)W, (cuuint64_t)H};
     const cuuint64_t strides[1] = {(cuuint64_t)W * sizeof(float)};
-    const cuuint32_t box[2] = {(cuuint32_t)(TW + 2 * RA + 4), (cuuint32_t)(TH + 2 * r)};
+    const cuuint32_t box[2] = {(cuuint32_t)(TW + 2 * RA + 4), (cuuint32_t)(th + 2 * r)};
     const cuuint32_t es[2] = {1, 1};
     const CUresult e = enc(&p.ref_map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(ref), dims, strides, box,
                            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
@@ -42,13 +42,14 @@ static bool make_ref_map(SweepParams& p, const float* ref, int H, int W, int r) 
     return e == CUDA_SUCCESS;
 }
 
-template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP>
-__global__ void __launch_bounds__(NT, 2) sweep_kernel(const __grid_constant__ SweepParams p) {
+template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP, int TH = TH_DEFAULT>
+__global__ void __launch_bounds__(TileShape<TH>::NT, TileShape<TH>::MIN_CTAS)
+    sweep_kernel(const __grid_constant__ SweepParams p) {
     extern __shared__ __align__(128) float4 smem4[];
     const int pa = p.i0 + blockIdx.z * p.ppc;
     const int pb = min(p.i1, pa + p.ppc);
-    sweep_tile<R, KMAX, PLANES, F16, true, true, X64, CMP>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
-                                                 p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
+    sweep_tile<R, KMAX, PLANES, F16, true, true, X64, CMP, TH>(p, blockIdx.x * TW, blockIdx.y * TH, pa, pb,
+                                                     p.rec ? (int)blockIdx.z : -1, reinterpret_cast<float*>(smem4));
 }
 
 __global__ void merge_kernel(long long HW, int nchunks, int i0, int i1, int ppc, const float* __restrict__ rec,
@@ -95,35 +96,43 @@ __global__ void finalize_kernel(int H, int W, int kind, int n, int t0, const flo
 
 // ------------------------------------------------------------------------------ launcher
 
-template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP>
+template <int R, int KMAX, bool PLANES, bool F16, bool X64, bool CMP, int TH>
 static mvs_status launch_sweep(const SweepParams& p, dim3 grid, cudaStream_t st) {
-    auto kern = sweep_kernel<R, KMAX, PLANES, F16, X64, CMP>;
-    const size_t smem = Geom<R>::smem_bytes() + (CMP ? Geom<R>::count_bytes() : 0);
+    auto kern = sweep_kernel<R, KMAX, PLANES, F16, X64, CMP, TH>;
+    const size_t smem = Geom<R, TH>::smem_bytes() + (CMP ? Geom<R, TH>::count_bytes() : 0);
     // the attribute is per function and per device: set it for the current device every time
     MVS_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
              "sweep: shared memory attribute");
-    kern<<<grid, NT, smem, st>>>(p);
+    kern<<<grid, TileShape<TH>::NT, smem, st>>>(p);
     return check_launch("sweep kernel");
 }
 
-template <int KMAX, bool PLANES, bool F16, bool X64 = false, bool CMP = false>
+template <int KMAX, bool PLANES, bool F16, bool X64 = false, bool CMP = false, int TH = TH_DEFAULT>
 static mvs_status dispatch_r(int r, const SweepParams& p, dim3 grid, cudaStream_t st) {
     switch (r) {
-        case 0: return launch_sweep<0, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 1: return launch_sweep<1, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 2: return launch_sweep<2, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 3: return launch_sweep<3, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 4: return launch_sweep<4, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 5: return launch_sweep<5, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 6: return launch_sweep<6, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
-        case 7: return launch_sweep<7, KMAX, PLANES, F16, X64, CMP>(p, grid, st);
+        case 0: return launch_sweep<0, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 1: return launch_sweep<1, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 2: return launch_sweep<2, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 3: return launch_sweep<3, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 4: return launch_sweep<4, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 5: return launch_sweep<5, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 6: return launch_sweep<6, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
+        case 7: return launch_sweep<7, KMAX, PLANES, F16, X64, CMP, TH>(p, grid, st);
     }
     return fail(MVS_ERR_VALUE, "sweep: window radius %d outside 0..%d", r, MVS_MAX_RADIUS);
 }
 
-static mvs_status dispatch(int r, int kmax, bool planes, int precision, const SweepParams& p, dim3 grid,
+static mvs_status dispatch(int r, int kmax, bool planes, int precision, int th, const SweepParams& p, dim3 grid,
                            cudaStream_t st) {
     const bool f16 = precision == MVS_PREC_FP16 || precision == MVS_PREC_FP16_COMP;
+    if (th != TH_DEFAULT) {   // the other tile shapes: FP32 / FP16-storage plane sweeps, 2-entry lists
+        if (!planes || kmax > 2 || (precision != MVS_PREC_FP32 && precision != MVS_PREC_FP16))
+            return fail(MVS_ERR_UNSUPPORTED, "sweep: tile height %d needs an FP32 or FP16 plane sweep with top_k <= 2", th);
+        if (th == 16) return f16 ? dispatch_r<2, true, true, false, false, 16>(r, p, grid, st)
+                                 : dispatch_r<2, true, false, false, false, 16>(r, p, grid, st);
+        return f16 ? dispatch_r<2, true, true, false, false, 64>(r, p, grid, st)
+                   : dispatch_r<2, true, false, false, false, 64>(r, p, grid, st);
+    }
     if (precision == MVS_PREC_FP32_COMP || precision == MVS_PREC_FP16_COMP) {
         if (!planes || kmax > 2) return fail(MVS_ERR_UNSUPPORTED, "sweep: compensated sums need MVS_HYP_PLANES and top_k <= 2");
         return f16 ? dispatch_r<2, true, true, false, true>(r, p, grid, st)
@@ -159,6 +168,13 @@ mvs_status validate_sweep(const mvs_sweep_args* a) {
     if (a->i1 < a->i0) return fail(MVS_ERR_VALUE, "sweep: empty or reversed hypothesis range");
     if (a->precision < MVS_PREC_FP32 || a->precision > MVS_PREC_FP16_COMP)
         return fail(MVS_ERR_VALUE, "sweep: unknown precision");
+    if (a->tile_h != 0 && a->tile_h != 16 && a->tile_h != 32 && a->tile_h != 64)
+        return fail(MVS_ERR_VALUE, "sweep: tile height %d is not 0, 16, 32 or 64", a->tile_h);
+    if (tile_height(a) != TH_DEFAULT &&
+        (a->hyp.kind != MVS_HYP_PLANES || (a->precision != MVS_PREC_FP32 && a->precision != MVS_PREC_FP16) ||
+         (a->top_k < a->n_src ? a->top_k : a->n_src) > 2))
+        return fail(MVS_ERR_UNSUPPORTED, "sweep: tile height %d needs an FP32 or FP16 plane sweep with top_k <= 2",
+                    a->tile_h);
     const int kind = a->hyp.kind;
     if (kind < MVS_HYP_MAPS || kind > MVS_HYP_PLANES) return fail(MVS_ERR_VALUE, "sweep: unknown hypothesis kind");
     if (a->H == 0 || a->W == 0) return MVS_OK;
@@ -276,13 +292,14 @@ mvs_status sweep_range(const mvs_sweep_args* a, int i0, int i1, float* rec_ws, i
         p.hyp_a = a->hyp.maps + (long long)(i0 - a->i0) * p.map_stride;
     }
     p.ppc = (n + nchunks - 1) / nchunks;
-    p.ref_tma = make_ref_map(p, a->ref, a->H, a->W, a->r) ? 1 : 0;
+    const int th = tile_height(a);
+    p.ref_tma = make_ref_map(p, a->ref, a->H, a->W, a->r, th) ? 1 : 0;
     const int used = (n + p.ppc - 1) / p.ppc;
     p.rec = used > 1 ? rec_ws : nullptr;
     p.nchunks = used;
     p.r = a->r;
-    dim3 grid((a->W + TW - 1) / TW, (a->H + TH - 1) / TH, used);
-    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision, p, grid, st));
+    dim3 grid((a->W + TW - 1) / TW, (a->H + th - 1) / th, used);
+    MVS_TRY(dispatch(a->r, kmax, a->hyp.kind == MVS_HYP_PLANES, a->precision, th, p, grid, st));
     if (used > 1) {
         const long long HW = (long long)a->H * a->W;
         merge_kernel<<<(unsigned)((HW + 255) / 256), 256, 0, st>>>(HW, used, i0, i1, p.ppc, rec_ws, a->best, a->prev,
@@ -294,7 +311,8 @@ mvs_status sweep_range(const mvs_sweep_args* a, int i0, int i1, float* rec_ws, i
 
 // Bytes of chunk-record scratch one sweep call needs (0 when a single chunk suffices).
 size_t sweep_scratch_bytes(const mvs_sweep_args* a, int* nchunks_out) {
-    const int tiles = ((a->W + TW - 1) / TW) * ((a->H + TH - 1) / TH);
+    const int th = tile_height(a);
+    const int tiles = ((a->W + TW - 1) / TW) * ((a->H + th - 1) / th);
     const int nplanes = a->i1 - a->i0;
     const int per_call = nplanes < MVS_MAX_PLANES_PER_CALL ? nplanes : MVS_MAX_PLANES_PER_CALL;
     int nch = a->plane_chunks > 0 ? a->plane_chunks : auto_plane_chunks(tiles, per_call);

@@ -34,10 +34,19 @@
 namespace mvs {
 
 constexpr int TW = 64;                 // output tile width (columns)
-constexpr int TH = 32;                 // output tile height (rows)
-constexpr int NT = 256;                // threads per CTA
-constexpr int SEG = NT / TW;           // row segments in stage C
-constexpr int ROWS = TH / SEG;         // output rows per thread in stage C
+constexpr int ROWS = 8;                // output rows per thread in stage C
+constexpr int TH_DEFAULT = 32;         // output tile height of the default shape
+
+// A TW x TH output tile runs on NT = 8 TH threads: thread t keeps column t mod TW and the ROWS rows
+// of segment t / TW in stage C, so every thread's rows start on a multiple of 8 in each of the
+// three shapes (TH = 16, 32, 64; 128, 256, 512 threads).
+template <int TH>
+struct TileShape {
+    static_assert(TH == 16 || TH == 32 || TH == 64, "tile height 16, 32 or 64");
+    static constexpr int NT = 8 * TH;              // threads per CTA
+    static constexpr int SEG = NT / TW;            // row segments (= TH / ROWS)
+    static constexpr int MIN_CTAS = TH == 16 ? 3 : (TH == 32 ? 2 : 1);   // resident CTAs per SM
+};
 
 struct SrcGeo {
     const void* img;                   // float or __half, (h, w) row-major
@@ -86,7 +95,7 @@ struct Coef {
     int pad_[3];
 };
 
-template <int R>
+template <int R, int TH = TH_DEFAULT>
 struct Geom {
     static constexpr int K = 2 * R + 1;
     static constexpr int RA = (R + 3) & ~3;        // halo rounded up to a float4
@@ -106,17 +115,17 @@ struct Geom {
 };
 
 // Largest shared-memory footprint over radii 0..RMAX (a persistent CTA serves any of them).
-template <int RMAX>
+template <int RMAX, int TH = TH_DEFAULT>
 constexpr size_t smem_bytes_upto() {
     size_t m = 0;
-    if constexpr (RMAX >= 0) m = Geom<0>::smem_bytes() > m ? Geom<0>::smem_bytes() : m;
-    if constexpr (RMAX >= 1) m = Geom<1>::smem_bytes() > m ? Geom<1>::smem_bytes() : m;
-    if constexpr (RMAX >= 2) m = Geom<2>::smem_bytes() > m ? Geom<2>::smem_bytes() : m;
-    if constexpr (RMAX >= 3) m = Geom<3>::smem_bytes() > m ? Geom<3>::smem_bytes() : m;
-    if constexpr (RMAX >= 4) m = Geom<4>::smem_bytes() > m ? Geom<4>::smem_bytes() : m;
-    if constexpr (RMAX >= 5) m = Geom<5>::smem_bytes() > m ? Geom<5>::smem_bytes() : m;
-    if constexpr (RMAX >= 6) m = Geom<6>::smem_bytes() > m ? Geom<6>::smem_bytes() : m;
-    if constexpr (RMAX >= 7) m = Geom<7>::smem_bytes() > m ? Geom<7>::smem_bytes() : m;
+    if constexpr (RMAX >= 0) m = Geom<0, TH>::smem_bytes() > m ? Geom<0, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 1) m = Geom<1, TH>::smem_bytes() > m ? Geom<1, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 2) m = Geom<2, TH>::smem_bytes() > m ? Geom<2, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 3) m = Geom<3, TH>::smem_bytes() > m ? Geom<3, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 4) m = Geom<4, TH>::smem_bytes() > m ? Geom<4, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 5) m = Geom<5, TH>::smem_bytes() > m ? Geom<5, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 6) m = Geom<6, TH>::smem_bytes() > m ? Geom<6, TH>::smem_bytes() : m;
+    if constexpr (RMAX >= 7) m = Geom<7, TH>::smem_bytes() > m ? Geom<7, TH>::smem_bytes() : m;
     return m;
 }
 
@@ -307,9 +316,9 @@ __device__ inline void make_coef_group(Coef& c, const SrcGeo& g, float inv, int 
 // Stage B: horizontal window sums of (V, J, J^2, J I) for one 16-column row segment per thread:
 // products formed once per input, running sums along the segment, one float4 per output.
 // WITHV = false when every sample is valid: the count column is not formed (it would be k).
-template <int R, bool WITHV>
+template <int R, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4* sH, int tid) {
-    using G = Geom<R>;
+    using G = Geom<R, TH>;
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
     // consecutive threads take consecutive rows of one segment: a quarter-warp's 16-byte loads then
@@ -363,7 +372,7 @@ __device__ __forceinline__ void stage_b(const float* sJ, const float* sI, float4
 
 // Stage C for one thread: vertical running sums down column c (rows y0 .. y0 + ROWS - 1), ZNCC,
 // insertion into the per-pixel top-k lists. WITHV = false: every window count is k^2.
-template <int R, int KMAX, bool WITHV>
+template <int R, int KMAX, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const float* mu, const float* rsd,
                                         float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
     constexpr int K = 2 * R + 1;
@@ -374,7 +383,7 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
-    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
+    MVS_BOUND(y0 + ROWS + 2 * R <= (Geom<R, TH>::HR) && c < TW);
     float cv = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
 #pragma unroll
     for (int t = 0; t < K; ++t) {
@@ -427,9 +436,9 @@ __device__ __forceinline__ void stage_c(const float4* sH, int c, int y0, const f
 // On bright low-texture windows, where the NCC divides by sd_ref * sd_src ~ 1e-3, float32 running
 // sums differ from the reference by up to ~1e-3; these track it to the last float32 bit or so.
 
-template <int R, bool WITHV>
+template <int R, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, float4* sH, int tid) {
-    using G = Geom<R>;
+    using G = Geom<R, TH>;
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
     const int sg = tid / HR, hy = tid - sg * HR;
@@ -480,7 +489,7 @@ __device__ __forceinline__ void stage_b64(const float* sJ, const float* sI, floa
 }
 
 // `sdv` holds the reference's window deviation itself (not its reciprocal) in this mode.
-template <int R, int KMAX, bool WITHV>
+template <int R, int KMAX, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const float* mu, const float* sdv,
                                           float (&topk)[ROWS][KMAX], float* total, bool bottom, int nlist) {
     constexpr int K = 2 * R + 1;
@@ -490,7 +499,7 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
-    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
+    MVS_BOUND(y0 + ROWS + 2 * R <= (Geom<R, TH>::HR) && c < TW);
     float cv = 0.f;
     double cj = 0.0, cjj = 0.0, cji = 0.0;
 #pragma unroll
@@ -553,9 +562,9 @@ __device__ __forceinline__ void stage_c64(const float4* sH, int c, int y0, const
 // windows are full and E[I'] = mu' exactly, so the last term is zero and is not formed; otherwise
 // the masked sum of I' is accumulated as a fifth quantity (the counts then move to a byte array).
 
-template <int R, bool WITHV>
+template <int R, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_b_cmp(const float* sJ, const float* sI, float4* sH, unsigned char* sV, int tid) {
-    using G = Geom<R>;
+    using G = Geom<R, TH>;
     constexpr int RA = G::RA, HR = G::HR, JP = G::JP, P = G::P, NSEG = G::NSEG, NIN = G::NIN;
     if (tid >= HR * NSEG) return;
     const int sg = tid / HR, hy = tid - sg * HR;
@@ -623,7 +632,7 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float x) {
 
 // `mu` holds the pivoted window mean mu' = mu - p and `rsd` the reciprocal window deviation, both
 // formed from the pivoted reference tile.
-template <int R, int KMAX, bool WITHV>
+template <int R, int KMAX, bool WITHV, int TH = TH_DEFAULT>
 __device__ __forceinline__ void stage_c_cmp(const float4* sH, const unsigned char* sV, int c, int y0, const float* mu,
                                             const float* rsd, float pv, float (&topk)[ROWS][KMAX], float* total,
                                             bool bottom, int nlist) {
@@ -634,7 +643,7 @@ __device__ __forceinline__ void stage_c_cmp(const float4* sH, const unsigned cha
 #pragma unroll
     for (int k = 0; k < 8; ++k) sw[k] = c ^ (((c >> 4) + k) & 7);
     const float4* col = sH + y0 * TW;
-    MVS_BOUND(y0 + ROWS + 2 * R <= Geom<R>::HR && c < TW);
+    MVS_BOUND(y0 + ROWS + 2 * R <= (Geom<R, TH>::HR) && c < TW);
     const unsigned char* ccol = sV + y0 * TW + c;
     float cv = 0.f, ci = 0.f, cj = 0.f, cjj = 0.f, cji = 0.f;
     float ej = 0.f, ejj = 0.f, eji = 0.f;            // Kahan compensations
@@ -750,9 +759,10 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // REF_TMA: the reference tile arrives by TMA when p.ref_tma is set (the single-view kernel, whose
 // parameters hold the tensor map; `smem` must then be 128-byte aligned).
 template <int R, int KMAX, bool PLANES, bool F16, bool WIDE = false, bool REF_TMA = false, bool X64 = false,
-          bool CMP = false>
+          bool CMP = false, int TH = TH_DEFAULT>
 __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb, int chunk, float* smem) {
-    using G = Geom<R>;
+    using G = Geom<R, TH>;
+    constexpr int NT = TileShape<TH>::NT, SEG = TileShape<TH>::SEG;
     constexpr int K = G::K, RA = G::RA, HR = G::HR, HC = G::HC, JP = G::JP, P = G::P, NSEG = G::NSEG,
                   NIN = G::NIN;
     float* sI = smem;                                  // HR x JP reference (0 outside); TMA destination
@@ -1007,39 +1017,39 @@ __device__ void sweep_tile(const SweepParams& p, int tx, int ty, int pa, int pb,
             // thread: products once per input, running sums along the segment
             if constexpr (CMP) {
                 if (all_valid) {
-                    stage_b_cmp<R, false>(sJ, sI, sH, sV, tid);
+                    stage_b_cmp<R, false, TH>(sJ, sI, sH, sV, tid);
                 } else {
-                    stage_b_cmp<R, true>(sJ, sI, sH, sV, tid);
+                    stage_b_cmp<R, true, TH>(sJ, sI, sH, sV, tid);
                 }
             } else if constexpr (X64) {
                 if (all_valid) {
-                    stage_b64<R, false>(sJ, sI, sH, tid);
+                    stage_b64<R, false, TH>(sJ, sI, sH, tid);
                 } else {
-                    stage_b64<R, true>(sJ, sI, sH, tid);
+                    stage_b64<R, true, TH>(sJ, sI, sH, tid);
                 }
             } else if (all_valid) {
-                stage_b<R, false>(sJ, sI, sH, tid);
+                stage_b<R, false, TH>(sJ, sI, sH, tid);
             } else {
-                stage_b<R, true>(sJ, sI, sH, tid);
+                stage_b<R, true, TH>(sJ, sI, sH, tid);
             }
             __syncthreads();
             // ---- C: vertical running sums down the column, NCC, top-k insertion
             if constexpr (CMP) {
                 if (all_valid) {
-                    stage_c_cmp<R, KMAX, false>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
+                    stage_c_cmp<R, KMAX, false, TH>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
                 } else {
-                    stage_c_cmp<R, KMAX, true>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
+                    stage_c_cmp<R, KMAX, true, TH>(sH, sV, c, seg * ROWS, mu, rsd, pv, topk, total, bottom, nlist);
                 }
             } else if constexpr (X64) {
                 if (all_valid) {
-                    stage_c64<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                    stage_c64<R, KMAX, false, TH>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
                 } else {
-                    stage_c64<R, KMAX, true>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                    stage_c64<R, KMAX, true, TH>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
                 }
             } else if (all_valid) {
-                stage_c<R, KMAX, false>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                stage_c<R, KMAX, false, TH>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
             } else {
-                stage_c<R, KMAX, true>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
+                stage_c<R, KMAX, true, TH>(sH, c, seg * ROWS, mu, rsd, topk, total, bottom, nlist);
             }
         }
         // ---- winner-take-all update for hypothesis i
@@ -1132,6 +1142,7 @@ __device__ __forceinline__ float finalize_pixel(float inv0, float inv1, int n, f
 }
 
 // host-side helpers shared by sweep.cu and batch.cu
+inline int tile_height(const mvs_sweep_args* a) { return a->tile_h ? a->tile_h : TH_DEFAULT; }
 mvs_status validate_sweep(const mvs_sweep_args* a);
 mvs_status fill_params(const mvs_sweep_args* a, SweepParams& p);
 int pick_kmax(SweepParams& p);

@@ -154,7 +154,7 @@ class Hypotheses:
 
 
 def sweep_args(ref, mu, sd, ray, srcs, geo, ref_cam, hyp: Hypotheses, r, top_k, state, i0=0, i1=None,
-               precision=L.PREC_FP32, plane_chunks=0):
+               precision=L.PREC_FP32, plane_chunks=0, tile_h=0):
     """Fills an mvs_sweep_args for device tensors (no copies). Returns (args, keepalive)."""
     a = L.SweepArgs()
     a.H, a.W = int(ref.shape[0]), int(ref.shape[1])
@@ -179,7 +179,7 @@ def sweep_args(ref, mu, sd, ray, srcs, geo, ref_cam, hyp: Hypotheses, r, top_k, 
     a.hyp = hyp.c()
     a.i0 = int(i0)
     a.i1 = int(hyp.n if i1 is None else i1)
-    a.r, a.top_k, a.plane_chunks = int(r), int(top_k), int(plane_chunks)
+    a.r, a.top_k, a.plane_chunks, a.tile_h = int(r), int(top_k), int(plane_chunks), int(tile_h)
     best, prev, spb, snb, idx = state
     a.best, a.prev, a.s_prev_best, a.s_next_best, a.idx = (best.data_ptr(), prev.data_ptr(), spb.data_ptr(),
                                                           snb.data_ptr(), idx.data_ptr())
@@ -194,14 +194,16 @@ def new_state(H: int, W: int, device=None):
 
 
 def sweep(ref, mu, sd, ray, srcs, geo, hyp: Hypotheses, r: int, top_k: int, state=None, ref_cam=None,
-          precision=L.PREC_FP32, plane_chunks: int = 0, stream=None):
+          precision=L.PREC_FP32, plane_chunks: int = 0, stream=None, tile_h: int = 0):
     """All hypotheses of ``hyp`` in one call on device tensors; returns the state tuple
-    (best, prev, s_prev_best, s_next_best, idx), updated in place when given."""
+    (best, prev, s_prev_best, s_next_best, idx), updated in place when given. tile_h: rows of the
+    kernel's 64-column output tiles (0 = 32; 16 and 64 for FP32 / FP16 plane sweeps with
+    top_k <= 2); it changes the float32 rounding of the plane maps, not the arithmetic."""
     H, W = int(ref.shape[0]), int(ref.shape[1])
     if state is None:
         state = new_state(H, W, ref.device)
     a, keep = sweep_args(ref, mu, sd, ray, srcs, geo, ref_cam, hyp, r, top_k, state, precision=precision,
-                         plane_chunks=plane_chunks)
+                         plane_chunks=plane_chunks, tile_h=tile_h)
     L.check(L.load().mvs_sweep(C_addr(a), L.stream_handle(stream)), "sweep")
     del keep
     return state

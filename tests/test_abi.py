@@ -111,6 +111,20 @@ def test_validation_errors_need_no_device():
     j.hyp.kind = L.HYP_PLANES
     assert lib.mvs_batch_create(ctypes.addressof(jobs), 1, None, ctypes.byref(h)) == L.ERR_UNSUPPORTED
     assert "single-view" in L.last_error()
+    # tile heights: 0 (= 32), 16, 32, 64; 16 and 64 only for FP32 / FP16 plane sweeps, top_k <= 2
+    c = L.SweepArgs()
+    c.n_src, c.r, c.top_k, c.geo, c.tile_h = 1, 1, 1, geo.ctypes.data, 48
+    assert lib.mvs_sweep(ctypes.addressof(c), None) == L.ERR_VALUE
+    assert "tile height 48" in L.last_error()
+    c.tile_h = 64                                  # per-pixel hypotheses: the default shape only
+    assert lib.mvs_sweep(ctypes.addressof(c), None) == L.ERR_UNSUPPORTED
+    c.hyp.kind, c.precision = L.HYP_PLANES, L.PREC_FP64_SUMS
+    assert lib.mvs_sweep(ctypes.addressof(c), None) == L.ERR_UNSUPPORTED
+    c.precision, c.tile_h = L.PREC_FP32, 16
+    assert lib.mvs_sweep(ctypes.addressof(c), None) == L.OK     # valid (an empty image: no work)
+    tun = L.BatchTuning(0, 0, 24)
+    assert lib.mvs_batch_create(ctypes.addressof(jobs), 1, ctypes.addressof(tun), ctypes.byref(h)) == L.ERR_VALUE
+    assert "tile height 24" in L.last_error()
 
 
 def test_depth_map_keeps_only_the_float64_sums_mode_on_per_pixel_sweeps():
