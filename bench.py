@@ -58,13 +58,19 @@ def parse():
     ap.add_argument("--jobs", type=int, default=64)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (jobs/s)")
     ap.add_argument("--serve-precision", choices=["fp32", "fp16"], default="fp16")
+    ap.add_argument("--check", action="store_true",
+                    help="the cpu_baseline leg also validates a %d-row band of the last timed step's sweep against "
+                         "the reference's CPU kernels (the parity tests' bar)" % CHECK_ROWS)
     ap.add_argument("--tile-h", type=int, choices=[0, 16, 32, 64], default=0,
                     help="rows of the sweep's 64-column output tiles (0 = 32)")
     ap.add_argument("--no-modes", action="store_true",
                     help="headline only: skip the batched (config 4) and served (config 5) summaries that a "
                          "1-GPU run appends to its line")
     ap.add_argument("--seed", type=int, default=0)
-    return ap.parse_args()
+    a = ap.parse_args()
+    if a.check and a.no_cpu:
+        ap.error("--check runs in the cpu_baseline leg: drop --no-cpu")
+    return a
 
 
 def workload(a):
@@ -253,6 +259,20 @@ def run_ours(a):
     if world > 1:
         dist.all_reduce(ms, op=dist.ReduceOp.MAX)
     ms_total = float(ms.item())
+    # --check: one row band of the last timed step's sweep (its state is untouched by PatchMatch),
+    # with the step's window statistics, for the cpu_baseline leg
+    band_out = None
+    if a.check and rank == 0:
+        y0c = max(r, (H // 2) // 32 * 32)
+        y1c = min(H - r, y0c + CHECK_ROWS)
+        dchk = torch.empty((H, W), dtype=torch.float32, device=dev)
+        h_ = hyp.c()
+        L.check(lib.mvs_sweep_finalize(H, W, ctypes.addressof(h_), state[0].data_ptr(), state[2].data_ptr(),
+                                       state[3].data_ptr(), state[4].data_ptr(), dchk.data_ptr(), sh))
+        torch.cuda.synchronize()
+        band_out = (y0c, y1c, state[4][y0c:y1c].cpu().numpy(), state[0][y0c:y1c].cpu().numpy(),
+                    dchk[y0c:y1c].cpu().numpy(), mu[y0c - r:y1c + r].cpu().numpy(), sd[y0c - r:y1c + r].cpu().numpy())
+        del dchk
     sweep_evals = H * W * nplanes * nsrc
     pm_evals = H * W * iters * PM_HYPS * nsrc
     evals = sweep_evals + pm_evals
@@ -398,6 +418,8 @@ def run_ours(a):
                               prec)
     if rank == 0 and not a.no_cpu:
         line["cpu_baseline"] = cpu_baseline(cfg, nplanes, iters, device=dev)   # sample rendered on the GPU
+        if band_out is not None:
+            line["cpu_baseline"]["check"] = reference_band_check(sc, ref_h, srcs_h, geo, planes, r, top_k, band_out)
     if world == 1 and a.mode == "headline" and not a.no_modes:
         line.update(mode_summaries(a, dev))
     if world > 1:
@@ -599,6 +621,74 @@ class CpuSample:
 
 def cpu_baseline(cfg, nplanes, iters, device="cpu"):
     return CpuSample(cfg, nplanes, iters, device=device).measure()
+
+
+CHECK_ROWS = 64        # rows of the timed step's sweep that --check validates
+
+
+def reference_band_check(sc, ref_h, srcs_h, geo, planes, r, top_k, band):
+    """--check (part of the cpu_baseline leg): rows [y0, y1) of the last timed step's sweep against
+    the reference's own CPU kernels (oracle/_ref: _dense.sweep_hypothesis over the same planes, on
+    every host core in row strips with their window halo; the oracle's C restatement when the
+    reference was not built), with the GPU step's own window statistics (mvs_ref_stats, bit-exact
+    with the reference's box filter). The bar of the parity tests: the winner index exact wherever
+    best - second best > 1e-3, index flips (near-ties) on at most 0.5 % of the pixels, depth
+    within 0.1 % on every pixel whose index matches (flipped pixels: counted, worst error given),
+    scores within 2e-4 where the index matches."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import oracle as O
+    R = O.reference()
+    kern = R._dense.sweep_hypothesis if R is not None else O.sweep_hypothesis
+    y0, y1, g_idx, g_best, g_depth, mu_b, sd_b = band        # mu_b / sd_b: rows [y0 - r, y1 + r)
+    H, W = ref_h.shape
+    cores = os.cpu_count() or 1
+    rows = -(-(y1 - y0) // cores)
+    parts = [(a_, min(y1, a_ + rows)) for a_ in range(y0, y1, rows)]
+
+    def part(pt):
+        a_, b_ = pt
+        s0, s1 = a_ - r, b_ + r                                   # rows the windows of [a_, b_) read
+        rr = np.ascontiguousarray(ref_h[s0:s1])
+        mm = np.ascontiguousarray(mu_b[s0 - (y0 - r): s1 - (y0 - r)])
+        ss = np.ascontiguousarray(sd_b[s0 - (y0 - r): s1 - (y0 - r)])
+        ry = O.rays_world((s1 - s0, W), _CropCam(sc.ref_cam, 0, s0, W, s1 - s0))
+        st = O.init_state(s1 - s0, W)
+        t1 = np.full((s1 - s0, W), -np.inf, np.float32)
+        t2 = np.full((s1 - s0, W), -np.inf, np.float32)
+        for i, pl in enumerate(planes):
+            kern(rr, mm, ss, srcs_h, ry, geo, np.full((s1 - s0, W), pl, np.float32), r, top_k, i, *st)
+            hi = np.maximum(t1, st[1])                             # st[1]: hypothesis i's scores
+            t2 = np.maximum(t2, np.minimum(t1, st[1]))
+            t1 = hi
+        k0, k1 = a_ - s0, b_ - s0
+        return [x[k0:k1] for x in st] + [(t1 - t2)[k0:k1]]
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(cores) as ex:
+        res = list(ex.map(part, parts))
+    secs = time.perf_counter() - t0
+    best, _, spb, snb, idx, gap = (np.concatenate([q[k] for q in res]) for k in range(6))
+    n = len(planes)
+    p0 = np.full(idx.shape, planes[0], np.float32)
+    p1 = np.full(idx.shape, planes[1] if n > 1 else planes[0], np.float32)
+    depth = O.finalize(best, spb, snb, idx, p0, p1, n).astype(np.float64)
+    decided = gap > 1e-3
+    same = g_idx == idx
+    fin = np.isfinite(depth) & (depth > 0)
+    rel = np.zeros(depth.shape)
+    rel[fin] = np.abs(g_depth.astype(np.float64)[fin] - depth[fin]) / depth[fin]
+    kept, flipped = fin & same, fin & ~same
+    score_err = np.abs(g_best.astype(np.float64) - best)[same]
+    out = {"rows": [int(y0), int(y1)], "pixels": int(idx.size), "kind": "reference" if R is not None else "port",
+           "cpu_s": round(secs, 2), "decided": int(decided.sum()), "decided_missed": int((decided & ~same).sum()),
+           "flips": int((~same).sum()),
+           "depth_rel_max_kept": float(rel[kept].max()) if kept.any() else 0.0,
+           "flip_depth_over_0.1pct": int((flipped & (rel > 1e-3)).sum()),
+           "score_abs_max_kept": float(score_err.max()) if score_err.size else 0.0}
+    out["pass"] = bool(out["decided_missed"] == 0 and out["flips"] <= 5e-3 * idx.size
+                       and out["depth_rel_max_kept"] <= 1e-3 and out["score_abs_max_kept"] <= 2e-4
+                       and np.array_equal(np.isfinite(g_depth) & fin, fin))
+    return out
 
 
 # ------------------------------------------------------------------ reference arm

@@ -546,6 +546,9 @@ __global__ void __launch_bounds__(256) pm_quad_kernel(const float* __restrict__ 
 #ifndef PM_LANE_MIN_BLOCKS
 #define PM_LANE_MIN_BLOCKS 4
 #endif
+#ifndef PM_LANE_MIN_BLOCKS_TRIALS
+#define PM_LANE_MIN_BLOCKS_TRIALS PM_LANE_MIN_BLOCKS
+#endif
 #ifndef PM_UNIT_INLINE
 #define PM_UNIT_INLINE __forceinline__
 #endif
@@ -869,7 +872,8 @@ __host__ __device__ inline int pm_side(int r, int step) { return (2 * r) / step 
 
 // PHASE 0: current plane and propagation; PHASE 1: the random trials.
 template <int L, int NSIDE, int PHASE>
-__global__ void __launch_bounds__(256, PM_LANE_MIN_BLOCKS) pm_lane_kernel(const __grid_constant__ PMParams c) {
+__global__ void __launch_bounds__(256, PHASE == 0 ? PM_LANE_MIN_BLOCKS : PM_LANE_MIN_BLOCKS_TRIALS)
+    pm_lane_kernel(const __grid_constant__ PMParams c) {
     extern __shared__ float4 pm_win[];
     const int H = c.H, W = c.W;
     const int lane = threadIdx.x & (L - 1);
