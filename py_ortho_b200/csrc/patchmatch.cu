@@ -538,13 +538,13 @@ __global__ void __launch_bounds__(256) pm_quad_kernel(const float* __restrict__ 
 // Float32 costs differ from the float64 ones by ~1e-7 (measured 99.9th percentile 2e-6), so the
 // strict '<' can decide near-ties differently; the float64 mode is the bit-exact reference.
 
-// samples of a window row unrolled in the unchecked window sums (0: the whole row)
-// Resident blocks of 256 threads per SM for the lane kernel. 4 (64 registers, a few spills)
-// measured 5 % faster than 3 (80 registers, no spills) on B200: 58.7 vs 61.7 ms for 2 iterations
-// of a 2000 x 1500, 8-source case; rolling or partly unrolling a window row's samples (smaller
-// code) was slower (64.3 / 62.4 ms).
+// Resident blocks of 256 threads per SM for the lane kernel (propagation; trials). On B200, 2 iterations
+// of a 2000 x 1500, 8-source case with one 16-byte footprint load per sample: 5 / 5 blocks (48
+// registers, spills) 54.4 ms, 4 / 5 55.2 ms, 4 / 4 (64 registers) 55.5 ms, 4 / 3 57.4 ms, 3 / 4
+// 58.6 ms. (With four scalar tap loads 4 blocks had been best: 58.7 ms against 61.7 ms at 3 and
+// 64.5 ms at 5; rolling or partly unrolling a window row's samples was slower.)
 #ifndef PM_LANE_MIN_BLOCKS
-#define PM_LANE_MIN_BLOCKS 4
+#define PM_LANE_MIN_BLOCKS 5
 #endif
 #ifndef PM_LANE_MIN_BLOCKS_TRIALS
 #define PM_LANE_MIN_BLOCKS_TRIALS PM_LANE_MIN_BLOCKS
