@@ -951,13 +951,87 @@ def serve_summary(a, dev, rate, precision="fp32", flight_data=None):
     return line
 
 
+def precision_summary(a, dev, seeds=10):
+    """Config 3 at its shape: config 1's view (640 x 480, 4 sources, 128 planes over [35, 55] m,
+    5 x 5, best 2) on ten seeded scenes, each window-sum / storage form swept on the device and
+    timed with CUDA events; then the checker, on the host cores: the oracle's all-float64 sweep of
+    the same planes (float64 statistics, sums, NCC and parabola), and each form's depth error
+    against it over all pixels (median, p99, p99.9, max)."""
+    import torch
+    from concurrent.futures import ThreadPoolExecutor
+    from py_ortho_b200 import _lib as L, dense, fast, scene as S
+    forms = {"fp32": L.PREC_FP32, "fp16": L.PREC_FP16, "fp32_comp": L.PREC_FP32_COMP, "fp16_comp": L.PREC_FP16_COMP,
+             "fp64_sums": L.PREC_FP64_SUMS}
+    planes = S.plane_list(35.0, 55.0, 128)
+    r, top_k = 2, 2
+    hyp = dense.Hypotheses.planes_inv(planes)
+    scenes, ms = [], {k: 0.0 for k in forms}
+    st = torch.cuda.current_stream()
+    for seed in range(seeds):
+        sc = S.make_scene("c1", seed=100 + seed, device=dev)
+        ref, srcs = sc.grey(sc.ref), [sc.grey(x) for x in sc.srcs]
+        geo = S.geo_rows(sc.ref_cam, sc.src_cams)
+        ref_d = torch.from_numpy(ref).to(dev)
+        mu, sd = fast.ref_stats(ref_d, r)
+        s32 = [torch.from_numpy(x).to(dev) for x in srcs]
+        s16 = [fast.to_fp16(x) for x in s32]
+        outs = {}
+        for name, prec in forms.items():
+            ss = s16 if prec in (L.PREC_FP16, L.PREC_FP16_COMP) else s32
+            for rep_ in range(2):                     # the first call warms the instance
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(st)
+                state = dense.sweep(ref_d, mu, sd, None, ss, geo, hyp, r, top_k, ref_cam=sc.ref_cam.row(),
+                                    precision=prec)
+                e1.record(st)
+                e1.synchronize()
+            ms[name] += e0.elapsed_time(e1)
+            outs[name] = dense.finalize(hyp, state).cpu().numpy().astype(np.float64)
+        scenes.append((sc, ref, srcs, geo, outs))
+    # the checker: the oracle's all-float64 sweep (host cores)
+    from oracle import oracle as O
+
+    def oracle64(item):
+        sc, ref, srcs, geo, _ = item
+        H, W = ref.shape
+        d64, _, _ = O.sweep_fp64(ref, srcs, O.rays_world((H, W), sc.ref_cam), geo,
+                                 [np.full((H, W), p, np.float64) for p in planes], r, top_k)
+        return d64
+
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(min(seeds, os.cpu_count() or 1)) as ex:
+        d64s = list(ex.map(oracle64, scenes))
+    cpu_s = time.perf_counter() - t0
+    H, W = scenes[0][1].shape
+    evals = seeds * H * W * len(planes) * len(scenes[0][2])
+    report = {}
+    for name in forms:
+        e = np.concatenate([(np.abs(item[4][name] - d64) / d64).ravel() for item, d64 in zip(scenes, d64s)])
+        nonfinite = int((~np.isfinite(e)).sum())
+        e = e[np.isfinite(e)]
+        report[name] = {"nonfinite": nonfinite, "median": float(np.median(e)), "p99": float(np.percentile(e, 99)),
+                        "p999": float(np.percentile(e, 99.9)), "max": float(e.max()),
+                        "within_0.1pct": float((e <= 1e-3).mean()),
+                        "ms_per_scene": round(ms[name] / seeds, 3), "evals_per_s": evals / (ms[name] / 1e3)}
+    return {"mode": "precision", "metric": "depth relative error vs the all-float64 oracle sweep",
+            "scenes": seeds, "forms": report, "oracle_cpu_s": round(cpu_s, 1),
+            "config": {"workload": "c3: c1's view 640x480, 4 sources, 128 planes over [35, 55] m, 5x5, best 2, "
+                                   "10 seeded scenes"}}
+
+
 def mode_summaries(a, dev):
-    """Config 4 (64 uneven views: per-view launches vs one persistent launch in a CUDA graph, FP32
+    """Config 3 (the precision forms' depth error at config 1's shape against the all-float64
+    oracle), config 4 (64 uneven views: per-view launches vs one persistent launch in a CUDA graph, FP32
     and FP16 storage) and config 5 (the FP16 continuous-batching server against the plain FP32
     per-request kernel at 20 and 200 jobs/s, 10 % PatchMatch jobs), appended to a 1-GPU headline
     line after its timed region. A failure is reported in the line instead of ending the run."""
     import torch
     out = {}
+    try:
+        out["c3_precision"] = precision_summary(a, dev)
+    except Exception as e:            # noqa: BLE001 - reported, the headline stands
+        out["c3_precision"] = {"error": f"{type(e).__name__}: {e}"}
+    torch.cuda.empty_cache()
     try:
         out["c4_batched"] = batch_summary(a, dev)
     except Exception as e:            # noqa: BLE001 - reported, the headline stands
