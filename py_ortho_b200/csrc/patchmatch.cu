@@ -566,21 +566,50 @@ __device__ __forceinline__ unsigned pmf_floor_bits(float x, float& f) {   // |x|
     return (unsigned)__float_as_int(t);
 }
 
-// Window statistics shared by the lanes of a pixel group, fixed for one visit.
-struct PMWin {
-    const float4* w;      // NW samples (ray_q - ray_p, I - mI; I = NaN: no sample), then 4 corners
-    int nw;               // samples in the window
+// A pixel's window as the cost code reads it: sample (row, k) = e-th of the window as
+// (ray_q - ray_p, I_q - mI) with I = NaN where there is no sample (outside the image or a
+// non-finite reference value), and the ray offsets of the clipped window's four corners.
+//   PMWinStaged: staged once per visit in shared memory by the pixel's lane group;
+//   PMWinTile:   read from the warp's shared tile of raw rays and reference values (one lane per
+//                pixel), the offsets formed on each read - the same float32 operations, so the
+//                same values (positions outside the image hold masked samples either way).
+struct PMWinStaged {
+    const float4* w;      // NW samples, then the 4 corners
+    __device__ __forceinline__ float4 at(int, int, int e) const { return w[e]; }
+    __device__ __forceinline__ float4 corner(int k4, int nw) const { return w[nw + k4]; }
+};
+struct PMWinTile {
+    const float4* t;      // tile entry of the window's first sample (row y - r, column x - r)
+    int rs, cs;           // tile offsets of one window row and one window column
+    int cy0, cy1, cx0, cx1;   // tile offsets of the clipped corners' rows and columns
+    float rpx, rpy, rpz, mI;
+    __device__ __forceinline__ float4 at(int row, int k, int) const {
+        const float4 v = t[row * rs + k * cs];
+        return make_float4(v.x - rpx, v.y - rpy, v.z - rpz, v.w - mI);
+    }
+    __device__ __forceinline__ float4 corner(int k4, int) const {
+        const float4 v = t[(k4 < 2 ? cy0 : cy1) + ((k4 & 1) ? cx1 : cx0)];
+        return make_float4(v.x - rpx, v.y - rpy, v.z - rpz, 0.f);
+    }
+};
+
+// Window statistics of a pixel, fixed for one visit.
+template <class Acc>
+struct PMWinT {
+    Acc acc;
+    int side, nw;         // samples along a side, in the window
     float nfin;           // samples with a finite reference value inside the image
     float si, sii;        // sum of (I - mI) and (I - mI)^2 over those samples
     bool allfin;          // every sample has a finite reference value inside the image
 };
+using PMWin = PMWinT<PMWinStaged>;
 
 // One source's window sums. CHECKED: every sample tested as in the reference (camera depth,
 // source bounds, finite value) and the reference sums formed per source; otherwise (the whole
 // window maps inside the source, no sample near a test) only the three source sums are formed.
 // ALLFIN: no reference sample is missing (no masking of the reference terms).
-template <int NSIDE, bool CHECKED, bool ALLFIN>
-__device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const float* A, const float* B,
+template <int NSIDE, bool CHECKED, bool ALLFIN, class Acc>
+__device__ __forceinline__ void pm_window_sums(const Acc& win, int side_rt, const float* A, const float* B,
                                                const float* C, float a0, float b0, float c0, float n0, float n1,
                                                float n2, float denp, float lou, float hiu, float lov, float hiv,
                                                unsigned kb, const float4* qd, int sw, unsigned last,
@@ -589,13 +618,12 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
                                                float& ns) {
     // rows rolled, the samples of a row unrolled when the side is known (the checked form, rare,
     // stays rolled to keep the instruction footprint small)
-    const int side = NSIDE > 0 ? NSIDE : 1;
-    const int NW = NSIDE > 0 ? NSIDE * NSIDE : nw;
+    const int side = NSIDE > 0 ? NSIDE : side_rt;
 #pragma unroll 1
-    for (int e0 = 0; e0 < NW; e0 += side)
+    for (int row = 0; row < side; ++row)
 #pragma unroll((NSIDE > 0 && !CHECKED) ? NSIDE : 1)
-    for (int e = e0; e < e0 + side; ++e) {
-        const float4 w = win[e];
+    for (int k = 0; k < side; ++k) {
+        const float4 w = win.at(row, k, row * side + k);
         const float cq = fmaf(C[0], w.x, fmaf(C[1], w.y, fmaf(C[2], w.z, c0)));
         const float aq = fmaf(A[0], w.x, fmaf(A[1], w.y, fmaf(A[2], w.z, a0)));
         const float bq = fmaf(B[0], w.x, fmaf(B[1], w.y, fmaf(B[2], w.z, b0)));
@@ -642,13 +670,14 @@ __device__ __forceinline__ void pm_window_sums(const float4* win, int nw, const 
 // float32 NCC of one (candidate, source) unit: plane (d, n) at the window's pixel, source s
 // (s < S); n . ray_p = ndr < -1e-6. Follows _pm_cost: -1 below the count gate, 0 below the
 // variance floor.
-template <int NSIDE>
-__device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
-                                            const double* n, double ndr, int sl) {
+template <int NSIDE, class Acc>
+__device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWinT<Acc>& wn, float rpx, float rpy, float rpz,
+                                            double d, const double* n, double ndr, int sl) {
     const double num = d * ndr;
     const float n0 = (float)n[0], n1 = (float)n[1], n2 = (float)n[2], denp = (float)ndr;
     const int NW = NSIDE > 0 ? NSIDE * NSIDE : wn.nw;
-    const float4* win = wn.w;
+    const Acc& win = wn.acc;
+    const int SIDE = NSIDE > 0 ? NSIDE : wn.side;
     // ---- per (candidate, source) local map. The camera point of sample q is M ray_q / (n.ray_q),
     // M = b n^T + num R. The window centre is formed in float64 (b (n.ray_p) + num R ray_p), the
     // rows of M (which only multiply ray_q - ray_p) in float32.
@@ -699,7 +728,7 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     int out_lo_u = 0, out_hi_u = 0, out_lo_v = 0, out_hi_v = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-        const float4 w = win[NW + k];
+        const float4 w = win.corner(k, NW);
         const float den = fmaf(n0, w.x, fmaf(n1, w.y, fmaf(n2, w.z, denp)));
         const float cq = fmaf(C[0], w.x, fmaf(C[1], w.y, fmaf(C[2], w.z, c0)));
         const float aq = fmaf(A[0], w.x, fmaf(A[1], w.y, fmaf(A[2], w.z, a0)));
@@ -738,10 +767,10 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     bool checked = !den_ok;                   // the count of samples needs the per-sample test
     if (!outside && inside) {
         if (wn.allfin) {
-            pm_window_sums<NSIDE, false, true>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+            pm_window_sums<NSIDE, false, true>(win, SIDE, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
                                                kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
         } else {
-            pm_window_sums<NSIDE, false, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+            pm_window_sums<NSIDE, false, false>(win, SIDE, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
                                                 kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
         }
         // a non-finite source value in the window poisons the sums: redo the source checked
@@ -755,7 +784,7 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
     }
     if (checked) {
         T1 = T2 = X = S1 = S2 = cnt = ns = 0.f;
-        pm_window_sums<NSIDE, true, false>(win, NW, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
+        pm_window_sums<NSIDE, true, false>(win, SIDE, A, B, C, a0, b0, c0, n0, n1, n2, denp, lou, hiu, lov, hiv,
                                            kb, qd, sw, (unsigned)last, mJ, T1, T2, X, S1, S2, cnt, ns);
     }
     // samples counted by the reference (finite reference value, n.ray_q < -1e-9): with every
@@ -779,8 +808,8 @@ __device__ PM_UNIT_INLINE float pm_unit_ncc(const PMParams& c, const PMWin& wn, 
 
 // float32 photo term (top-k mean NCC) of plane (d, n): the L lanes of a pixel group evaluate one
 // source each and sort their NCCs with a shuffle network; every lane returns the same value.
-template <int L, int NSIDE>
-__device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz, double d,
+template <int L, int NSIDE, class Acc>
+__device__ float pm_photo_lane(const PMParams& c, const PMWinT<Acc>& wn, float rpx, float rpy, float rpz, double d,
                                const double* n, double ndr, int s, unsigned gmask) {
     float ncc = s < c.S ? pm_unit_ncc<NSIDE>(c, wn, rpx, rpy, rpz, d, n, ndr, s) : -INFINITY;   // idle lanes sort last
     // ---- descending bitonic sort over the group, then the mean of the first top_k
@@ -803,8 +832,8 @@ __device__ float pm_photo_lane(const PMParams& c, const PMWin& wn, float rpx, fl
 
 // float32 photo term of plane (d, n) evaluated by one lane over all sources (the propagation
 // step gives each lane its own candidate); the top-k list is kept sorted in registers.
-template <int NSIDE, int KM>
-__device__ __forceinline__ float pm_photo_cand_k(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+template <int NSIDE, int KM, class Acc>
+__device__ __forceinline__ float pm_photo_cand_k(const PMParams& c, const PMWinT<Acc>& wn, float rpx, float rpy, float rpz,
                                                  double d, const double* n, double ndr) {
     const int kk = c.top_k < c.S ? c.top_k : c.S;
     float top[KM];
@@ -828,18 +857,18 @@ __device__ __forceinline__ float pm_photo_cand_k(const PMParams& c, const PMWin&
     return sum / (float)kk;
 }
 
-template <int NSIDE>
-__device__ __noinline__ float pm_photo_cand_wide(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+template <int NSIDE, class Acc>
+__device__ __noinline__ float pm_photo_cand_wide(const PMParams& c, const PMWinT<Acc>& wn, float rpx, float rpy, float rpz,
                                                  double d, const double* n, double ndr) {
-    return pm_photo_cand_k<NSIDE, MVS_MAX_SOURCES>(c, wn, rpx, rpy, rpz, d, n, ndr);
+    return pm_photo_cand_k<NSIDE, MVS_MAX_SOURCES, Acc>(c, wn, rpx, rpy, rpz, d, n, ndr);
 }
 
 // top_k <= 2 (the reference's default) keeps a 2-entry list; wider lists take an out-of-line call
-template <int NSIDE>
-__device__ __forceinline__ float pm_photo_cand(const PMParams& c, const PMWin& wn, float rpx, float rpy, float rpz,
+template <int NSIDE, class Acc>
+__device__ __forceinline__ float pm_photo_cand(const PMParams& c, const PMWinT<Acc>& wn, float rpx, float rpy, float rpz,
                                                double d, const double* n, double ndr) {
-    if (c.top_k <= 2) return pm_photo_cand_k<NSIDE, 2>(c, wn, rpx, rpy, rpz, d, n, ndr);
-    return pm_photo_cand_wide<NSIDE>(c, wn, rpx, rpy, rpz, d, n, ndr);
+    if (c.top_k <= 2) return pm_photo_cand_k<NSIDE, 2, Acc>(c, wn, rpx, rpy, rpz, d, n, ndr);
+    return pm_photo_cand_wide<NSIDE, Acc>(c, wn, rpx, rpy, rpz, d, n, ndr);
 }
 
 // Geometric term over the group: lane s contributes source s's error (float64, as pm_geo).
@@ -906,7 +935,8 @@ __global__ void __launch_bounds__(256, PHASE == 0 ? PM_LANE_MIN_BLOCKS : PM_LANE
     MVS_BOUND((threadIdx.x / L + 1) * (nw + 4) * sizeof(float4) <= c.win_smem);
     const float rpx = __ldg(c.ray + idx), rpy = __ldg(c.ray + HW + idx), rpz = __ldg(c.ray + 2 * HW + idx);
     PMWin wn;
-    wn.w = win;
+    wn.acc.w = win;
+    wn.side = side;
     wn.nw = nw;
     {
         float sum = 0.f, k = 0.f;
@@ -1078,6 +1108,162 @@ __global__ void __launch_bounds__(256, PHASE == 0 ? PM_LANE_MIN_BLOCKS : PM_LANE
     c.flags[t] = (unsigned char)((isfinite(dcur) ? 1u : 0u) | ((unsigned)changed << 1));
 }
 
+// ---------------------------------------------------------------- float32 trials, one lane per pixel
+//
+// In pm_lane_kernel the trials' lanes are the sources, and a pixel is seen by only some of them
+// (5.1 of 8 on average in a 3 x 3 flight at 60-75 % overlap): the other lanes idle. Here a warp
+// takes 32 consecutive pixels of one colour in one row and each lane evaluates its own pixel's
+// two trials over all sources, as propagation evaluates its candidates; neighbouring pixels see
+// the same sources, so the lanes skip the same ones together. The warp stages one tile of raw
+// rays and reference values (rows y - r .. y + r, columns x_first - r .. x_last + r: 2r + 1 rows
+// of 64 + 2r) in place of a window per pixel, and the window statistics are summed in the lane
+// kernel's order (L strided partial sums, then its butterfly), so a trial's cost has the lane
+// kernel's bits when top_k <= 2 and no source has a depth map (otherwise the top-k and geometric
+// sums add the same terms in another order).
+constexpr int PM_TRIAL_WARPS = 4;   // warps per block
+#ifndef PM_TRIAL_MIN_BLOCKS
+#define PM_TRIAL_MIN_BLOCKS 6
+#endif
+#ifndef PM_TRIAL_LANE_GROUPS
+#define PM_TRIAL_LANE_GROUPS 0      // 1: the trials on the lane groups' kernel (comparisons)
+#endif
+
+__host__ __device__ inline int pm_tile_pitch(int r) { return 64 + 2 * r; }
+__host__ __device__ inline size_t pm_tile_entries(int r) { return (size_t)(2 * r + 1) * pm_tile_pitch(r); }
+
+// Sums over the window's samples e = 0 .. nw - 1 as an L-lane group forms them: lane l adds
+// e = l, l + L, ... in order, then the xor butterfly (every lane ends with the same value).
+template <int L, class F>
+__device__ __forceinline__ void pm_group_sums(int nw, F&& term, float& a, float& b) {
+    float pa[L], pb[L];
+#pragma unroll
+    for (int l = 0; l < L; ++l) {
+        pa[l] = 0.f;
+        pb[l] = 0.f;
+        for (int e = l; e < nw; e += L) term(e, pa[l], pb[l]);
+    }
+#pragma unroll
+    for (int o = L >> 1; o > 0; o >>= 1)
+#pragma unroll
+        for (int l = 0; l < L; ++l)
+            if (!(l & o)) {
+                const float sa = pa[l] + pa[l | o], sb = pb[l] + pb[l | o];
+                pa[l] = sa; pa[l | o] = sa;
+                pb[l] = sb; pb[l | o] = sb;
+            }
+    a = pa[0];
+    b = pb[0];
+}
+
+template <int L, int NSIDE>
+__global__ void __launch_bounds__(32 * PM_TRIAL_WARPS, PM_TRIAL_MIN_BLOCKS)
+    pm_trial_kernel(const __grid_constant__ PMParams c) {
+    extern __shared__ float4 pm_tiles[];
+    const int H = c.H, W = c.W, r = c.r, step = c.step;
+    const int half_w = (W + 1) / 2, wpr = (half_w + 31) >> 5;            // warps per row
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long gw = (long long)blockIdx.x * PM_TRIAL_WARPS + warp;
+    if (gw >= (long long)H * wpr) return;                                 // the whole warp
+    const int y = (int)(gw / wpr), k0 = (int)(gw - (long long)y * wpr) * 32;
+    const int par = (y + c.colour) & 1;
+    const int pitch = pm_tile_pitch(r), rows = 2 * r + 1;
+    const int xs0 = 2 * k0 + par - r;                                     // image column of tile column 0
+    float4* tile = pm_tiles + (size_t)warp * rows * pitch;
+    MVS_BOUND((size_t)(warp + 1) * rows * pitch * sizeof(float4) <= c.win_smem);
+    const long long HW = (long long)H * W;
+    for (int e = lane; e < rows * pitch; e += 32) {
+        const int ty = e / pitch, tx = e - ty * pitch;
+        const int yy = y - r + ty, xx = xs0 + tx;
+        float4 v = make_float4(0.f, 0.f, 0.f, __int_as_float(0x7fc00000));
+        if (yy >= 0 && yy < H && xx >= 0 && xx < W) {
+            const long long q = (long long)yy * W + xx;
+            v.x = __ldg(c.ray + q);
+            v.y = __ldg(c.ray + HW + q);
+            v.z = __ldg(c.ray + 2 * HW + q);
+            const float I = __ldg(c.ref + q);
+            if (fabsf(I) <= 3.4e38f) v.w = I;
+        }
+        tile[e] = v;
+    }
+    __syncwarp();
+    const int k = k0 + lane, x = 2 * k + par;
+    if (k >= half_w || x >= W) return;
+    const long long t = (long long)y * half_w + k, idx = (long long)y * W + x;
+    if (!c.active[idx]) return;
+    const unsigned pflag = c.flags[t];
+    if (!(pflag & 1u)) {               // no draws: the visit ends with propagation's result
+        pm_finish(c, idx, c.depth[idx], c.pbest[t], c.psc[t], pflag >> 1);
+        return;
+    }
+    int ng = 0;
+    for (int s = 0; s < c.S; ++s) ng += c.dep[s] != nullptr;
+    const bool use_geo = c.geo_w > 0.0 && ng > 0;
+    const int side = NSIDE > 0 ? NSIDE : pm_side(r, step);
+    const int nw = side * side;
+    const float rpx = __ldg(c.ray + idx), rpy = __ldg(c.ray + HW + idx), rpz = __ldg(c.ray + 2 * HW + idx);
+    // this pixel's window in the tile: sample (row, col) at w0[row * step * pitch + col * step]
+    const float4* w0 = tile + 2 * lane;
+    const int rs = step * pitch;
+    float sum, kc, si, sii;
+    pm_group_sums<L>(nw, [&](int e, float& a, float& b) {
+        const int row = e / side, col = e - row * side;
+        const float I = w0[row * rs + col * step].w;
+        if (I == I) {
+            a += I;
+            b += 1.f;
+        }
+    }, sum, kc);
+    const float mI = kc > 0.f ? sum / kc : 0.f;
+    pm_group_sums<L>(nw, [&](int e, float& a, float& b) {
+        const int row = e / side, col = e - row * side;
+        const float I = w0[row * rs + col * step].w;
+        if (I == I) {
+            const float Ip = I - mI;
+            a += Ip;
+            b = fmaf(Ip, Ip, b);
+        }
+    }, si, sii);
+    PMWinT<PMWinTile> wn;
+    wn.acc.t = w0;
+    wn.acc.rs = rs;
+    wn.acc.cs = step;
+    wn.acc.cy0 = (max(y - r, 0) - (y - r)) * pitch;
+    wn.acc.cy1 = (min(y + r, H - 1) - (y - r)) * pitch;
+    wn.acc.cx0 = max(x - r, 0) - (x - r);
+    wn.acc.cx1 = min(x + r, W - 1) - (x - r);
+    wn.acc.rpx = rpx;
+    wn.acc.rpy = rpy;
+    wn.acc.rpz = rpz;
+    wn.acc.mI = mI;
+    wn.side = side;
+    wn.nw = nw;
+    wn.nfin = kc;
+    wn.si = si;
+    wn.sii = sii;
+    wn.allfin = kc == (float)nw;
+    const double rx = rpx, ry = rpy, rz = rpz;
+    auto cost = [&](double d, const double* nb, double& photo) -> double {
+        const double ndr = nb[0] * rx + nb[1] * ry + nb[2] * rz;
+        if (ndr >= -1e-6 || d <= 0.0) {
+            photo = 0.0;
+            return 10.0;
+        }
+        photo = (double)pm_photo_cand<NSIDE>(c, wn, rpx, rpy, rpz, d, nb, ndr);
+        const double geo = use_geo ? pm_geo(c, d, rx, ry, rz) : 0.0;
+        return (1.0 - photo) + c.geo_w * geo;
+    };
+    float dcur = c.depth[idx];
+    float ncur[3] = {c.normal[idx], c.normal[HW + idx], c.normal[2 * HW + idx]};
+    double best = c.pbest[t], sc = c.psc[t];
+    unsigned long long changed = pflag >> 1;
+    pm_trials(c, c.pstate[t], dcur, ncur, best, sc, changed, cost);
+    c.depth[idx] = dcur;
+    c.normal[idx] = ncur[0];
+    c.normal[HW + idx] = ncur[1];
+    c.normal[2 * HW + idx] = ncur[2];
+    pm_finish(c, idx, dcur, best, sc, changed);
+}
+
 }  // namespace mvs
 
 using namespace mvs;
@@ -1226,6 +1412,27 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
                 status = fail(MVS_ERR_CUDA, "pm_refine: shared-memory carve-out");
         }
     }
+    // the trials: one lane per pixel (pm_trial_kernel) when the warps' tiles fit in shared memory,
+    // else the lane groups' kernel
+    void (*trial_kernel)(PMParams) = nullptr;
+    const size_t smem_trial = (size_t)PM_TRIAL_WARPS * pm_tile_entries(a->r) * sizeof(float4);
+    const int wpr = (int)(((a->W + 1) / 2 + 31) / 32);
+    const unsigned grid_trial = (unsigned)(((long long)a->H * wpr + PM_TRIAL_WARPS - 1) / PM_TRIAL_WARPS);
+#if !PM_TRIAL_LANE_GROUPS
+    if (fast && status == MVS_OK && smem_trial <= 227 * 1024) {
+#define PM_PICK_TRIAL(LN)                                                                        \
+    trial_kernel = side == 7 ? pm_trial_kernel<LN, 7> : side == 5 ? pm_trial_kernel<LN, 5> : pm_trial_kernel<LN, 0>;
+        if (lanes == 4) { PM_PICK_TRIAL(4) }
+        else if (lanes == 8) { PM_PICK_TRIAL(8) }
+        else { PM_PICK_TRIAL(16) }
+#undef PM_PICK_TRIAL
+        if (cudaFuncSetAttribute(trial_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_trial) !=
+            cudaSuccess) {
+            cudaGetLastError();
+            trial_kernel = nullptr;
+        }
+    }
+#endif
     const unsigned grid = fast ? (unsigned)((n * lanes + block - 1) / block) : (unsigned)((n + 127) / 128);
     if (status == MVS_OK) {
         pm_rng_init_kernel<<<1, 1, 0, st>>>(rng, a->rng_state, a->seed | 1u);
@@ -1239,12 +1446,18 @@ extern "C" mvs_status mvs_pm_refine(const mvs_pm_args* a, void* stream) {
         p.nn_scale = 0.3 / (double)(git + 1);
         for (int colour = 0; colour < 2 && status == MVS_OK; ++colour) {
             p.colour = colour;
+            p.win_smem = (unsigned)smem;
             if (fast) lane_kernel[0]<<<grid, block, smem, st>>>(p);
             else pm_kernel<0><<<grid, 128, 0, st>>>(p);
             pm_count_kernel<<<nb, PM_SCAN_BLOCK, 0, st>>>(p.flags, n, bsum);
             pm_scan_kernel<<<1, PM_SCAN_BLOCK, 0, st>>>(bsum, nb, rng, cur, cur ^ 1, J);
             pm_state_kernel<<<nb, PM_SCAN_BLOCK, 0, st>>>(p.flags, n, bsum, rng, cur, J, pstate);
-            if (fast) lane_kernel[1]<<<grid, block, smem, st>>>(p);
+            if (trial_kernel) {
+                p.win_smem = (unsigned)smem_trial;
+                trial_kernel<<<grid_trial, 32 * PM_TRIAL_WARPS, smem_trial, st>>>(p);
+            } else if (fast) {
+                lane_kernel[1]<<<grid, block, smem, st>>>(p);
+            }
             else pm_kernel<1><<<grid, 128, 0, st>>>(p);
             cur ^= 1;
             status = check_launch("pm_refine kernels");
