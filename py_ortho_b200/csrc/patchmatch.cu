@@ -1120,9 +1120,12 @@ __global__ void __launch_bounds__(256, PHASE == 0 ? PM_LANE_MIN_BLOCKS : PM_LANE
 // kernel's order (L strided partial sums, then its butterfly), so a trial's cost has the lane
 // kernel's bits when top_k <= 2 and no source has a depth map (otherwise the top-k and geometric
 // sums add the same terms in another order).
+// Blocks of 4 warps; resident blocks per SM measured on B200 (2 iterations of a 2000 x 1500,
+// 8-source case, the whole PatchMatch call): 3 (168 registers) 50.9 ms, 4 (128) 50.1 ms, 5 (96,
+// spills) 53.0 ms, 6 (80) 52.6 ms, 8 (64) 57.6 ms; the lane groups' trials 54.0-54.4 ms.
 constexpr int PM_TRIAL_WARPS = 4;   // warps per block
 #ifndef PM_TRIAL_MIN_BLOCKS
-#define PM_TRIAL_MIN_BLOCKS 6
+#define PM_TRIAL_MIN_BLOCKS 4
 #endif
 #ifndef PM_TRIAL_LANE_GROUPS
 #define PM_TRIAL_LANE_GROUPS 0      // 1: the trials on the lane groups' kernel (comparisons)
