@@ -325,16 +325,17 @@ def run_ours(a):
                                    "frac": round(roof_sweep["evals_per_s"] / (issue_rate / SWEEP_INST_PER_EVAL), 4)}
     roof_pm = None
     if iters:
-        roof_pm = {"kernel": "pm_lane_kernel" if a.pm_precision == "fp32" else "pm_kernel",
+        roof_pm = {"kernel": "pm_lane_kernel + pm_trial_kernel" if a.pm_precision == "fp32" else "pm_kernel",
                    "precision": a.pm_precision,
                    "bound": "fp32-issue" if a.pm_precision == "fp32" else "fp64-issue",
                    "evals_per_s": pm_evals / (ms_pm / 1e3),
                    "ms": round(ms_pm, 3), "share_of_step": round(ms_pm / (ms_pm + ms_sweep), 4),
                    "ncu_profile": PM_PROFILE[a.pm_precision],
-                   "issue_active_ncu": ({"propagation": 0.711, "trials": 0.581} if a.pm_precision == "fp32"
+                   "issue_active_ncu": ({"propagation": 0.668, "trials": 0.505} if a.pm_precision == "fp32"
                                         else 0.667),
-                   "note": "not a contraction and not HBM-bound (DRAM < 1 %): bound by SIMT issue; "
-                           "issue_active is the fraction of SM issue slots used (ncu, see ncu_profile)"}
+                   "note": "not a contraction and not HBM-bound (DRAM < 2 %): propagation is bound by SIMT "
+                           "issue, the trials by latency at low occupancy; issue_active is the fraction of SM "
+                           "issue slots used (ncu, see ncu_profile)"}
     # the cost of the precision forms of the sweep, each timed once after the timed region on the
     # same view: compensated FP32 sums (config 3's form; FP16 sources), and the reference's float64
     # window sums
