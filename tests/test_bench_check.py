@@ -38,3 +38,16 @@ def test_band_check_passes_on_the_oracle_result_and_catches_a_planted_flip():
     idx[yy, xx] = (idx[yy, xx] + 3) % len(planes)
     out2 = bench.reference_band_check(sc, ref, srcs, geo, planes, r, top_k, (y0, y1, idx) + band[3:])
     assert not out2["pass"] and out2["decided_missed"] == 1
+
+
+def test_check_needs_the_cpu_baseline_leg():
+    """--check runs inside the cpu_baseline leg, so the bench refuses it together with --no-cpu
+    (an argument error, before any device work)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--check", "--no-cpu"], capture_output=True,
+                       text=True, timeout=300)
+    assert r.returncode == 2
+    assert "--check runs in the cpu_baseline leg" in r.stderr
